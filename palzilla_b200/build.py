@@ -1,0 +1,76 @@
+"""Builds the sm_100a CUDA library in-tree: palzilla_b200/libpalzilla_b200.so.
+
+Each translation unit is compiled with nvcc for sm_100a.  Units whose results must
+be bit-exact with the CPU oracle (BVH keys, traversal, photons, eye pass) are built
+with -fmad=false so that no multiply-add pair is contracted into an FMA; the solver
+units keep FMA contraction.  Objects are rebuilt only when a source or header is
+newer than the object.
+"""
+from __future__ import annotations
+
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libpalzilla_b200.so")
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+          "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]
+
+# translation unit -> extra flags
+UNITS = {
+    "pz_sort.cu": [],
+    "pz_bvh.cu": ["-fmad=false"],
+    "pz_capi.cu": [],
+}
+
+
+def _newer(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(verbose: bool = False, jobs: int | None = None) -> str:
+    os.makedirs(OBJ, exist_ok=True)
+    headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + \
+        glob.glob(os.path.join(ROOT, "include", "*.h"))
+    objs, procs = [], []
+    for unit, flags in UNITS.items():
+        src = os.path.join(CSRC, unit)
+        obj = os.path.join(OBJ, unit.replace(".cu", ".o"))
+        objs.append(obj)
+        if _newer(obj, [src] + headers + [__file__]):
+            cmd = [NVCC] + ARCH + COMMON + flags + ["-c", src, "-o", obj]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            procs.append((unit, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
+    failed = []
+    for unit, p in procs:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            failed.append(unit)
+            sys.stderr.write(out.decode())
+        elif verbose and out:
+            sys.stdout.write(out.decode())
+    if failed:
+        raise RuntimeError(f"nvcc failed for {failed}")
+    if _newer(LIB, objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcuda"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose="-v" in sys.argv)
+    print(LIB)

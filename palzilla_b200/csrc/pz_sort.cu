@@ -1,0 +1,284 @@
+// pz_sort.cu -- onesweep radix sort kernels (see pz_sort.cuh for the design).
+#include "pz_sort.cuh"
+
+namespace pz {
+namespace sort {
+
+// ---------------------------------------------------------------------------
+// histogram of every digit pass + look-back clear
+// ---------------------------------------------------------------------------
+template <class KeyT>
+__global__ void __launch_bounds__(kThreads) k_hist(const KeyT* __restrict__ keys, uint32_t n, int startBit,
+                                                   int nPasses, Header* __restrict__ h, unsigned long long* lookback,
+                                                   size_t lookbackWords)
+{
+    __shared__ uint32_t sh[kMaxPasses * kRadix];
+    for (int i = threadIdx.x; i < nPasses * kRadix; i += kThreads) sh[i] = 0;
+    __syncthreads();
+    clear_lookback(lookback, lookbackWords);
+
+    constexpr int kPerVec = 16 / sizeof(KeyT);
+    const uint32_t nVec = (reinterpret_cast<uintptr_t>(keys) & 15) ? 0u : n / kPerVec;
+    const uint4* v4 = reinterpret_cast<const uint4*>(keys);
+    const uint32_t stride = gridDim.x * kThreads;
+    for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < nVec; i += stride) {
+        uint4 q = __ldcs(v4 + i);
+        KeyT k[kPerVec];
+        memcpy(k, &q, 16);
+#pragma unroll
+        for (int e = 0; e < kPerVec; e++)
+            for (int p = 0; p < nPasses; p++) atomicAdd(&sh[p * kRadix + digit_of(k[e], startBit + 8 * p)], 1u);
+    }
+    for (uint32_t i = nVec * kPerVec + blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
+        KeyT k = keys[i];
+        for (int p = 0; p < nPasses; p++) atomicAdd(&sh[p * kRadix + digit_of(k, startBit + 8 * p)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nPasses * kRadix; i += kThreads) {
+        uint32_t c = sh[i];
+        if (c) atomicAdd(&h->hist[0][0] + i, c);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// one digit pass
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kFlagA = 1ull << 32;  // tile aggregate published
+constexpr unsigned long long kFlagP = 2ull << 32;  // inclusive prefix published
+
+PZ_D unsigned long long ld_volatile(const unsigned long long* p)
+{
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+PZ_D void st_volatile(unsigned long long* p, unsigned long long v)
+{
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Exclusive block-wide scan of one value per thread (256 threads); returns the
+// exclusive prefix.  `ws` is kWarps words of shared scratch.
+PZ_D uint32_t block_exclusive_scan(uint32_t x, uint32_t* ws)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) ws[warp] = inc;
+    __syncthreads();
+    uint32_t wpre = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; w++) wpre += (w < warp) ? ws[w] : 0u;
+    __syncthreads();
+    return wpre + inc - x;
+}
+
+template <class KeyT, bool kHasVal>
+struct PassSmem {
+    KeyT keys[kTile];
+    uint32_t vals[kHasVal ? kTile : 1];
+    uint16_t wcnt[kWarps][kRadix];   // per-warp digit counts, then per-warp exclusive offsets
+    uint32_t dstart[kRadix];         // tile-local exclusive digit start
+    uint32_t gbase[kRadix];          // global destination of the digit run minus dstart
+    uint32_t ws[2][kWarps];
+    uint32_t tile;
+};
+
+template <class KeyT, bool kHasVal>
+__global__ void __launch_bounds__(kThreads) k_pass(const KeyT* __restrict__ kin, KeyT* __restrict__ kout,
+                                                   const uint32_t* __restrict__ vin, uint32_t* __restrict__ vout,
+                                                   uint32_t n, int bit, int pass, Header* __restrict__ h,
+                                                   unsigned long long* __restrict__ lookback)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto& S = *reinterpret_cast<PassSmem<KeyT, kHasVal>*>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    if (tid == 0) S.tile = atomicAdd(&h->tile_counter[pass], 1u);
+    {
+        uint32_t* wc = reinterpret_cast<uint32_t*>(&S.wcnt[0][0]);
+        for (int i = tid; i < kWarps * kRadix / 2; i += kThreads) wc[i] = 0;
+    }
+    __syncthreads();
+    const uint32_t tile = S.tile;
+    const uint32_t base = tile * kTile;
+
+    // ---- load (warp-striped: warp w owns items [w*512, w*512+512) of the tile)
+    KeyT key[kItems];
+    uint32_t val[kHasVal ? kItems : 1];
+    const uint32_t wbase = base + warp * (kItems * 32);
+#pragma unroll
+    for (int k = 0; k < kItems; k++) {
+        uint32_t idx = wbase + k * 32 + lane;
+        if (idx < n) {
+            key[k] = __ldcs(kin + idx);
+            if (kHasVal) val[k] = __ldcs(vin + idx);
+        } else {
+            key[k] = 0;
+            if (kHasVal) val[k] = 0;
+        }
+    }
+
+    // ---- stable warp ranking, item order = (k, lane)
+    uint16_t rank[kItems];
+    const uint32_t ltmask = (1u << lane) - 1u;
+#pragma unroll
+    for (int k = 0; k < kItems; k++) {
+        const uint32_t idx = wbase + k * 32 + lane;
+        const bool valid = idx < n;
+        const uint32_t d = digit_of(key[k], bit);
+        uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            const bool set = (d >> b) & 1u;
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, set);
+            peers &= set ? bal : ~bal;
+        }
+        const uint32_t before = __popc(peers & ltmask);
+        const uint32_t cnt = valid ? S.wcnt[warp][d] : 0u;
+        __syncwarp();
+        if (valid && before == 0) S.wcnt[warp][d] = (uint16_t)(cnt + __popc(peers));
+        __syncwarp();
+        rank[k] = (uint16_t)(cnt + before);
+    }
+    __syncthreads();
+
+    // ---- per digit (thread = digit): warp offsets, tile total, tile-local start
+    const int d = tid;
+    uint32_t total = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; w++) {
+        uint32_t c = S.wcnt[w][d];
+        S.wcnt[w][d] = (uint16_t)total;
+        total += c;
+    }
+    const uint32_t gcount = h->hist[pass][d];
+    const uint32_t dstart = block_exclusive_scan(total, S.ws[0]);
+    const uint32_t gexcl = block_exclusive_scan(gcount, S.ws[1]);
+    S.dstart[d] = dstart;
+
+    // ---- decoupled look-back over earlier tiles for digit d
+    const unsigned long long tag = (unsigned long long)(pass + 1) << 34;
+    unsigned long long* mine = lookback + (size_t)tile * kRadix + d;
+    uint32_t prefix = 0;
+    if (tile == 0) {
+        st_volatile(mine, tag | kFlagP | total);
+    } else {
+        st_volatile(mine, tag | kFlagA | total);
+        int t = (int)tile - 1;
+        uint32_t spins = 0;
+        while (t >= 0) {
+            unsigned long long w = ld_volatile(lookback + (size_t)t * kRadix + d);
+            if ((w & ~0x3FFFFFFFFull) != tag || (w & (3ull << 32)) == 0) {
+                if (++spins > kSpinLimit) {
+                    raise_error(&h->status, kErrSpinLimit);
+                    break;
+                }
+                if (spins > 64) __nanosleep(64);
+                continue;
+            }
+            prefix += (uint32_t)w;
+            if (w & kFlagP) break;
+            t--;
+        }
+        st_volatile(mine, tag | kFlagP | (uint32_t)(prefix + total));
+    }
+    S.gbase[d] = gexcl + prefix - dstart;
+    __syncthreads();
+
+    // ---- scatter into shared memory in digit order
+#pragma unroll
+    for (int k = 0; k < kItems; k++) {
+        const uint32_t idx = wbase + k * 32 + lane;
+        if (idx < n) {
+            const uint32_t dd = digit_of(key[k], bit);
+            const uint32_t pos = S.dstart[dd] + S.wcnt[warp][dd] + rank[k];
+            S.keys[pos] = key[k];
+            if (kHasVal) S.vals[pos] = val[k];
+        }
+    }
+    __syncthreads();
+
+    // ---- write digit runs to their global positions
+    const uint32_t tileN = min((uint32_t)kTile, n - base);
+#pragma unroll 4
+    for (uint32_t i = tid; i < tileN; i += kThreads) {
+        const KeyT kk = S.keys[i];
+        const uint32_t dst = S.gbase[digit_of(kk, bit)] + i;
+        if (dst < n) {  // always true unless a look-back wait expired (status already set)
+            kout[dst] = kk;
+            if (kHasVal) vout[dst] = S.vals[i];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+template <class KeyT>
+cudaError_t launch_hist(const KeyT* keys, uint32_t n, int startBit, int nPasses, Header* h,
+                        unsigned long long* lookback, cudaStream_t s)
+{
+    int blocks = kNumSMs * kHistBlocksPerSM;
+    uint32_t need = (n + kThreads * 8 - 1) / (kThreads * 8);
+    if ((uint32_t)blocks > need) blocks = (int)(need > 0 ? need : 1);
+    k_hist<KeyT><<<blocks, kThreads, 0, s>>>(keys, n, startBit, nPasses, h, lookback,
+                                             (size_t)num_tiles(n) * kRadix);
+    return cudaGetLastError();
+}
+
+template <class KeyT, bool kHasVal>
+static cudaError_t launch_pass(const KeyT* kin, KeyT* kout, const uint32_t* vin, uint32_t* vout, uint32_t n, int bit,
+                               int pass, Header* h, unsigned long long* lookback, cudaStream_t s)
+{
+    const size_t smem = sizeof(PassSmem<KeyT, kHasVal>);
+    static bool configured = false;  // the attribute is per function, set once
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(k_pass<KeyT, kHasVal>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    k_pass<KeyT, kHasVal><<<num_tiles(n), kThreads, smem, s>>>(kin, kout, vin, vout, n, bit, pass, h, lookback);
+    return cudaGetLastError();
+}
+
+template <class KeyT>
+cudaError_t launch_passes(KeyT* keys, uint32_t* vals, KeyT* tmpKeys, uint32_t* tmpVals, uint32_t n, int startBit,
+                          int nPasses, Header* h, unsigned long long* lookback, cudaStream_t s)
+{
+    KeyT* src = keys;
+    KeyT* dst = tmpKeys;
+    uint32_t* vsrc = vals;
+    uint32_t* vdst = tmpVals;
+    for (int p = 0; p < nPasses; p++) {
+        cudaError_t e = vals ? launch_pass<KeyT, true>(src, dst, vsrc, vdst, n, startBit + 8 * p, p, h, lookback, s)
+                             : launch_pass<KeyT, false>(src, dst, nullptr, nullptr, n, startBit + 8 * p, p, h,
+                                                        lookback, s);
+        if (e != cudaSuccess) return e;
+        KeyT* t = src; src = dst; dst = t;
+        uint32_t* tv = vsrc; vsrc = vdst; vdst = tv;
+    }
+    if (src != keys) {  // odd number of passes: result is in tmp (tinyhiponesweep.h:659-667)
+        cudaError_t e = cudaMemcpyAsync(keys, src, sizeof(KeyT) * (size_t)n, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return e;
+        if (vals) e = cudaMemcpyAsync(vals, vsrc, sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+template cudaError_t launch_hist<uint32_t>(const uint32_t*, uint32_t, int, int, Header*, unsigned long long*, cudaStream_t);
+template cudaError_t launch_hist<unsigned long long>(const unsigned long long*, uint32_t, int, int, Header*,
+                                                     unsigned long long*, cudaStream_t);
+template cudaError_t launch_passes<uint32_t>(uint32_t*, uint32_t*, uint32_t*, uint32_t*, uint32_t, int, int, Header*,
+                                             unsigned long long*, cudaStream_t);
+template cudaError_t launch_passes<unsigned long long>(unsigned long long*, uint32_t*, unsigned long long*, uint32_t*,
+                                                       uint32_t, int, int, Header*, unsigned long long*, cudaStream_t);
+
+}  // namespace sort
+}  // namespace pz

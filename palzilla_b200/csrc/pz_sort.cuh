@@ -1,0 +1,74 @@
+// pz_sort.cuh -- onesweep LSD radix sort for sm_100a (8-bit digits).
+//
+// Behaviour of the reference sorter (tinyhiponesweep.h:592-668): a stable sort of
+// 32- or 64-bit keys on digit passes covering bits [startBit, startBit + 8 *
+// ceil((endBit - startBit) / 8)), optionally carrying a u32 value per key, with the
+// result ending in the caller's buffers.  Each digit is the full 8 bits at its
+// position (tinyhiponesweep.h:93-94), so a partial last digit also orders on the
+// bits above endBit, exactly as the reference does.
+//
+// Design (independent of the reference's kernels):
+//  * one histogram kernel computes every pass's digit counts in a single read and,
+//    in the same launch, clears the look-back table;
+//  * one kernel per pass: tiles of 4096 items claim a tile index from an atomic
+//    counter (so a tile only ever waits on tiles that are already running), rank
+//    keys stably with warp ballots, resolve the tile's global digit offsets with a
+//    decoupled look-back over 64-bit words {value, flag, pass tag}, stage the tile
+//    in shared memory in digit order and write digit runs out coalesced;
+//  * every spin wait is bounded; on expiry the kernel sets kErrSpinLimit in the
+//    status word and finishes (with undefined output) instead of hanging.
+#pragma once
+#include "pz_common.cuh"
+
+namespace pz {
+namespace sort {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kItems = 16;
+constexpr int kTile = kThreads * kItems;  // 4096 items per tile
+constexpr int kRadix = 256;
+constexpr int kMaxPasses = 8;
+constexpr int kHistBlocksPerSM = 4;
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+// Scratch header (the first kHeaderBytes of the sort scratch).
+struct Header {
+    uint32_t status;                       // kErr* bits
+    uint32_t pad0[31];
+    uint32_t tile_counter[kMaxPasses];
+    uint32_t pad1[32 - kMaxPasses];
+    uint32_t hist[kMaxPasses][kRadix];     // digit counts per pass
+};
+constexpr size_t kHeaderBytes = 16384;
+static_assert(sizeof(Header) <= kHeaderBytes, "header");
+
+inline uint32_t num_tiles(uint32_t n) { return (n + kTile - 1) / kTile; }
+inline int num_passes(int startBit, int endBit) { return (endBit - startBit + 7) / 8; }
+inline size_t lookback_bytes(uint32_t n) { return (size_t)num_tiles(n) * kRadix * sizeof(unsigned long long); }
+inline size_t scratch_bytes(uint32_t n) { return kHeaderBytes + ((lookback_bytes(n) + 255) & ~(size_t)255); }
+
+// Launch helpers (defined in pz_sort.cu).  `hist_done` means the histogram and the
+// look-back clear were already produced by a fused producer (the Morton kernel).
+template <class KeyT>
+cudaError_t launch_hist(const KeyT* keys, uint32_t n, int startBit, int nPasses, Header* h,
+                        unsigned long long* lookback, cudaStream_t s);
+template <class KeyT>
+cudaError_t launch_passes(KeyT* keys, uint32_t* vals, KeyT* tmpKeys, uint32_t* tmpVals, uint32_t n, int startBit,
+                          int nPasses, Header* h, unsigned long long* lookback, cudaStream_t s);
+
+// Device helpers shared with fused producers.
+template <class KeyT>
+PZ_D uint32_t digit_of(KeyT k, int bit) { return (uint32_t)(k >> bit) & 0xFFu; }
+
+// Clears `words` 64-bit look-back entries with a grid-stride loop (16-byte stores).
+PZ_D void clear_lookback(unsigned long long* lb, size_t words)
+{
+    size_t pairs = words / 2;
+    uint4* p = reinterpret_cast<uint4*>(lb);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < pairs; i += (size_t)gridDim.x * blockDim.x)
+        p[i] = make_uint4(0, 0, 0, 0);
+}
+
+}  // namespace sort
+}  // namespace pz

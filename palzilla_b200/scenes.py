@@ -1,0 +1,261 @@
+"""Seeded synthetic scenes for the caustics hot path.
+
+The reference renders an Alembic scene that is not part of its sources, so every
+workload here is generated: heightfield glass lenses over a receiver plane, a
+dispersive icosphere, random triangle soups for the sort/build benchmark and an
+uneven batch of lenses.  Each generator is deterministic for a given seed.
+
+Binary layouts match the reference's structs (minimum_lbvh.h:207-210,
+pk.h:74-78): a triangle is 9 float32 (36 B), an attribute record is one int32
+material followed by 9 float32 shading normals (40 B).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+MATERIAL_DIFFUSE = 0     # pk.h:67-72
+MATERIAL_MIRROR = 1
+MATERIAL_DIELECTRIC = 2
+
+ATTRIB_DTYPE = np.dtype([("material", "<i4"), ("ns", "<f4", (9,))])
+assert ATTRIB_DTYPE.itemsize == 40
+
+EV_T = 1  # event bit set = transmission (pk.h:117-121)
+
+
+def event_descriptor(events: str) -> int:
+    """EventDescriptor::asU32 (pk.h:122-162) of an event string such as "TT"."""
+    bits = 0
+    for i, c in enumerate(events):
+        if c == "T":
+            bits |= 1 << i
+        elif c != "R":
+            raise ValueError(f"bad event {c!r}")
+    return bits | (len(events) << 24)
+
+
+@dataclasses.dataclass
+class Camera:
+    eye: tuple
+    center: tuple
+    up: tuple
+    fovy: float  # radians
+
+
+@dataclasses.dataclass
+class Scene:
+    name: str
+    tris: np.ndarray      # (n, 9) float32
+    attribs: np.ndarray   # (n,) ATTRIB_DTYPE
+    p_light: tuple = (0.0, 3.0, 0.0)
+    camera: Camera | None = None
+    width: int = 256
+    height: int = 256
+    cauchy_a: float = 1.5
+    cauchy_b: float = 4200.0      # nm^2  (0.0042 um^2)
+    lambda_min: float = 380.0
+    lambda_max: float = 780.0
+    n_bins: int = 16
+    events: str = "T"
+    light_intensity: float = 16.0    # pk.h:1686
+    radiance_clamp: float = 12.0     # pk.h:1688
+    min_throughput: float = 0.05     # pk.h:1687
+    cell_step: float = 0.01          # pk.h:1376
+    photons_per_triangle: int = 256  # PHOTON_BLOCK_SIZE, pk.h:32
+    albedo: tuple = (0.75, 0.75, 0.75)
+
+    @property
+    def n(self) -> int:
+        return int(self.tris.shape[0])
+
+    def bin_lambdas(self) -> np.ndarray:
+        w = (self.lambda_max - self.lambda_min) / self.n_bins
+        return (self.lambda_min + (np.arange(self.n_bins, dtype=np.float64) + 0.5) * w).astype(np.float32)
+
+    def bin_etas(self) -> np.ndarray:
+        lam = self.bin_lambdas()
+        return (np.float32(self.cauchy_a) + np.float32(self.cauchy_b) / (lam * lam)).astype(np.float32)
+
+    def eta_range(self) -> tuple:
+        """(eta_min, eta_max) as the photon pass gets them: Cauchy at the short and
+        long ends of the band (pk.h:1448-1449)."""
+        a, b = np.float32(self.cauchy_a), np.float32(self.cauchy_b)
+        lo, hi = np.float32(self.lambda_min), np.float32(self.lambda_max)
+        return float(a + b / (lo * lo)), float(a + b / (hi * hi))
+
+
+def _attribs(normals: np.ndarray, material: int) -> np.ndarray:
+    a = np.zeros(normals.shape[0], dtype=ATTRIB_DTYPE)
+    a["material"] = material
+    a["ns"] = normals.reshape(-1, 9).astype(np.float32)
+    return a
+
+
+def receiver_plane(size: float, y: float = 0.0):
+    """Two diffuse triangles spanning [-size/2, size/2]^2 at height y, facing +y."""
+    h = size * 0.5
+    p = np.array([[-h, y, -h], [h, y, -h], [h, y, h], [-h, y, h]], dtype=np.float32)
+    # winding so that cross(v1 - v0, v2 - v0) points to +y
+    tris = np.stack([np.concatenate([p[0], p[2], p[1]]), np.concatenate([p[0], p[3], p[2]])]).astype(np.float32)
+    n = np.tile(np.array([0, 1, 0], np.float32), (2, 3, 1))
+    return tris, _attribs(n, MATERIAL_DIFFUSE)
+
+
+def heightfield_lens(side: int = 64, seed: int = 1, amplitude: float = 0.01, n_terms: int = 4,
+                     extent: float = 1.0, y: float = 1.0, material: int = MATERIAL_DIELECTRIC):
+    """Glass sheet over a side x side vertex grid spanning [-extent/2, extent/2]^2 at
+    height y; height is a sum of n_terms sinusoids with seeded frequency in [1, 6],
+    phase in [0, 2pi) and direction; shading normals are the analytic gradient normals."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    freq = rng.uniform(1.0, 6.0, n_terms)
+    phase = rng.uniform(0.0, 2.0 * math.pi, n_terms)
+    ang = rng.uniform(0.0, 2.0 * math.pi, n_terms)
+    amp = np.full(n_terms, amplitude) if np.isscalar(amplitude) else np.asarray(amplitude)
+    dx, dz = np.cos(ang), np.sin(ang)
+    g = np.linspace(-extent * 0.5, extent * 0.5, side, dtype=np.float64)
+    X, Z = np.meshgrid(g, g, indexing="xy")  # X varies along columns
+    arg = 2.0 * math.pi * freq[None, None, :] * (X[..., None] * dx + Z[..., None] * dz) + phase
+    H = y + (amp * np.sin(arg)).sum(-1)
+    dHdx = (amp * np.cos(arg) * 2.0 * math.pi * freq * dx).sum(-1)
+    dHdz = (amp * np.cos(arg) * 2.0 * math.pi * freq * dz).sum(-1)
+    P = np.stack([X, H, Z], -1)
+    N = np.stack([-dHdx, np.ones_like(H), -dHdz], -1)
+    N /= np.linalg.norm(N, axis=-1, keepdims=True)
+    i, j = np.meshgrid(np.arange(side - 1), np.arange(side - 1), indexing="xy")
+    i, j = i.ravel(), j.ravel()
+    a = (j, i); b = (j, i + 1); c = (j + 1, i + 1); d = (j + 1, i)
+    # quad a(x0,z0) b(x1,z0) c(x1,z1) d(x0,z1); winding a,d,b and b,d,c gives +y normals
+    t0 = np.stack([P[a], P[d], P[b]], 1)
+    t1 = np.stack([P[b], P[d], P[c]], 1)
+    n0 = np.stack([N[a], N[d], N[b]], 1)
+    n1 = np.stack([N[b], N[d], N[c]], 1)
+    tris = np.stack([t0, t1], 1).reshape(-1, 3, 3)
+    norms = np.stack([n0, n1], 1).reshape(-1, 3, 3)
+    return tris.reshape(-1, 9).astype(np.float32), _attribs(norms, material)
+
+
+def icosphere(subdivisions: int = 5, radius: float = 0.5, center=(0.0, 1.0, 0.0), material: int = MATERIAL_DIELECTRIC):
+    """Icosphere with 20 * 4^subdivisions triangles, outward winding, smooth normals."""
+    t = (1.0 + math.sqrt(5.0)) / 2.0
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+             (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+             (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    V = [np.array(v, np.float64) / np.linalg.norm(v) for v in verts]
+    F = list(faces)
+    for _ in range(subdivisions):
+        cache = {}
+
+        def mid(i, j):
+            key = (min(i, j), max(i, j))
+            if key not in cache:
+                m = V[i] + V[j]
+                V.append(m / np.linalg.norm(m))
+                cache[key] = len(V) - 1
+            return cache[key]
+
+        nf = []
+        for a, b, c in F:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        F = nf
+    Vn = np.array(V)
+    Fa = np.array(F)
+    P = Vn[Fa] * radius + np.asarray(center)
+    N = Vn[Fa]
+    # make every face wind outward
+    ng = np.cross(P[:, 1] - P[:, 0], P[:, 2] - P[:, 0])
+    flip = (ng * (P.mean(1) - np.asarray(center))).sum(-1) < 0
+    P[flip] = P[flip][:, [0, 2, 1]]
+    N[flip] = N[flip][:, [0, 2, 1]]
+    return P.reshape(-1, 9).astype(np.float32), _attribs(N, material)
+
+
+def random_soup(n: int, seed: int = 1001):
+    """n triangles: one vertex uniform in [0,1]^3 plus two edges of length U[1e-3, 1e-2]
+    in random directions (the sort + build workload)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    v0 = rng.random((n, 3), dtype=np.float32)
+    out = np.empty((n, 9), np.float32)
+    out[:, 0:3] = v0
+    for k in (1, 2):
+        d = rng.standard_normal((n, 3), dtype=np.float32)
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        ln = rng.uniform(1e-3, 1e-2, (n, 1)).astype(np.float32)
+        out[:, 3 * k:3 * k + 3] = v0 + d * ln
+    return out
+
+
+def _combine(parts):
+    tris = np.concatenate([p[0] for p in parts]).astype(np.float32)
+    att = np.concatenate([p[1] for p in parts])
+    return np.ascontiguousarray(tris), att
+
+
+def flat_sheet(side: int, y: float, extent: float = 1.0, facing: float = -1.0, material: int = MATERIAL_DIELECTRIC):
+    """Flat glass sheet (the bottom face of a two-surface lens), normals along facing*y."""
+    g = np.linspace(-extent * 0.5, extent * 0.5, side, dtype=np.float64)
+    X, Z = np.meshgrid(g, g, indexing="xy")
+    P = np.stack([X, np.full_like(X, y), Z], -1)
+    i, j = np.meshgrid(np.arange(side - 1), np.arange(side - 1), indexing="xy")
+    i, j = i.ravel(), j.ravel()
+    a = (j, i); b = (j, i + 1); c = (j + 1, i + 1); d = (j + 1, i)
+    if facing > 0:
+        t = np.stack([np.stack([P[a], P[d], P[b]], 1), np.stack([P[b], P[d], P[c]], 1)], 1)
+    else:
+        t = np.stack([np.stack([P[a], P[b], P[d]], 1), np.stack([P[b], P[c], P[d]], 1)], 1)
+    t = t.reshape(-1, 3, 3)
+    n = np.zeros_like(t)
+    n[..., 1] = facing
+    return t.reshape(-1, 9).astype(np.float32), _attribs(n, material)
+
+
+def lens_scene(side: int = 64, seed: int = 1, amplitude: float = 0.01, events: str = "T", n_bins: int = 16,
+               width: int = 256, height: int = 256, name: str | None = None) -> Scene:
+    """Heightfield-lens caustic: heightfield glass surface at y=1 over a 1x1 diffuse
+    receiver at y=0, point light at (0,3,0).  For "TT" the lens gets a flat bottom face
+    at y=0.92 (2 x 15 x 15 triangles), so paths refract twice.  The pinhole camera sits
+    between lens and receiver looking straight down, so eye paths reach the receiver
+    without crossing glass."""
+    parts = [heightfield_lens(side, seed, amplitude)]
+    eye_y = 0.9
+    if len(events) >= 2:
+        parts.append(flat_sheet(16, 0.92))
+        eye_y = 0.85
+    parts.append(receiver_plane(1.0, 0.0))
+    tris, att = _combine(parts)
+    fovy = 2.0 * math.atan(0.5 / eye_y)
+    cam = Camera(eye=(0.0, eye_y, 0.0), center=(0.0, 0.0, 0.0), up=(0.0, 0.0, -1.0), fovy=fovy)
+    return Scene(name=name or f"lens{side}", tris=tris, attribs=att, camera=cam, events=events, n_bins=n_bins,
+                 width=width, height=height)
+
+
+def sphere_scene(subdivisions: int = 5, n_bins: int = 64, width: int = 1024, height: int = 1024) -> Scene:
+    """Two-refraction dispersive sphere: icosphere r=0.5 at (0,1,0) over a 4x4 receiver at
+    y=0.  The light sits at (0,4,0) (centre of the 0.2 x 0.2 area light).  The camera at
+    y=0.45, below the sphere, looks down on the central 0.9 x 0.9 of the receiver where
+    the caustic falls."""
+    sph = icosphere(subdivisions)
+    tris, att = _combine([sph, receiver_plane(4.0, 0.0)])
+    cam = Camera(eye=(0.0, 0.45, 0.0), center=(0.0, 0.0, 0.0), up=(0.0, 0.0, -1.0), fovy=math.pi / 2)
+    return Scene(name=f"sphere{subdivisions}", tris=tris, attribs=att, p_light=(0.0, 4.0, 0.0), camera=cam,
+                 events="TT", n_bins=n_bins, width=width, height=height)
+
+
+def uneven_batch(n_scenes: int = 256, seed: int = 3001, side_min: int = 16, side_max: int = 256):
+    """Uneven batch: grid side log-uniform in [side_min, side_max], 1-2 refractions,
+    amplitude U[0.005, 0.03]."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    sides = np.exp(rng.uniform(math.log(side_min), math.log(side_max), n_scenes)).astype(int)
+    amps = rng.uniform(0.005, 0.03, n_scenes)
+    ks = rng.integers(1, 3, n_scenes)
+    scenes = []
+    for i in range(n_scenes):
+        s = lens_scene(int(sides[i]), seed=seed + 1 + i, amplitude=float(amps[i]), events="T" * int(ks[i]),
+                       n_bins=16, name=f"batch{i}")
+        scenes.append(s)
+    return scenes
