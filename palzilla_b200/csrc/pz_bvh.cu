@@ -18,6 +18,8 @@
 //    no 0xFF memset (every field of every node is written by the build);
 //  * the build launches ceil(n / 256) blocks over all n leaves (the reference launches
 //    ceil((n - 1) / 256) and so skips leaf n - 1 when n % 256 == 1).
+#include <cuda/atomic>
+
 #include "pz_bvh.cuh"
 #include "pz_sort.cuh"
 
@@ -59,33 +61,57 @@ PZ_D void stage_tris(float* sm, const Tri* tris, uint32_t first, uint32_t count)
 
 constexpr int kBlock = 256;
 
+// Streams the vertex array as 16-byte loads: 12 floats (4 vertices) per step, whose
+// axis pattern is fixed (x y z x | y z x y | z x y z).
 __global__ void __launch_bounds__(kBlock) k_scene_aabb(const Tri* __restrict__ tris, uint32_t n, Scratch* s)
 {
-    __shared__ __align__(16) float sm[kBlock * 9];
-    Box b = box_empty();
-    for (uint32_t first = blockIdx.x * kBlock; first < n; first += gridDim.x * kBlock) {
-        uint32_t cnt = min((uint32_t)kBlock, n - first);
-        __syncthreads();
-        stage_tris(sm, tris, first, cnt);
-        __syncthreads();
-        if (threadIdx.x < cnt) {
-            const float* t = sm + threadIdx.x * 9;
-            box_extend(b, mk3(t[0], t[1], t[2]));
-            box_extend(b, mk3(t[3], t[4], t[5]));
-            box_extend(b, mk3(t[6], t[7], t[8]));
-        }
+    const float* f = reinterpret_cast<const float*>(tris);
+    const uint64_t nf = (uint64_t)n * 9;
+    float lo[3] = {kFltMax, kFltMax, kFltMax}, hi[3] = {-kFltMax, -kFltMax, -kFltMax};
+    auto ext = [&](int a, float v) {
+        lo[a] = fminf(lo[a], v);
+        hi[a] = fmaxf(hi[a], v);
+    };
+    const bool aligned = (reinterpret_cast<uintptr_t>(f) & 15) == 0;
+    const uint64_t groups = aligned ? nf / 12 : 0;
+    const float4* q = reinterpret_cast<const float4*>(f);
+    const uint64_t stride = (uint64_t)gridDim.x * kBlock;
+    uint64_t g = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
+    for (; g + stride < groups; g += 2 * stride) {
+        const float4 a0 = __ldcs(q + 3 * g), b0 = __ldcs(q + 3 * g + 1), c0 = __ldcs(q + 3 * g + 2);
+        const uint64_t h = g + stride;
+        const float4 a1 = __ldcs(q + 3 * h), b1 = __ldcs(q + 3 * h + 1), c1 = __ldcs(q + 3 * h + 2);
+        ext(0, a0.x); ext(1, a0.y); ext(2, a0.z); ext(0, a0.w); ext(1, b0.x); ext(2, b0.y);
+        ext(0, b0.z); ext(1, b0.w); ext(2, c0.x); ext(0, c0.y); ext(1, c0.z); ext(2, c0.w);
+        ext(0, a1.x); ext(1, a1.y); ext(2, a1.z); ext(0, a1.w); ext(1, b1.x); ext(2, b1.y);
+        ext(0, b1.z); ext(1, b1.w); ext(2, c1.x); ext(0, c1.y); ext(1, c1.z); ext(2, c1.w);
     }
-    float v[6] = {b.lo.x, b.lo.y, b.lo.z, b.hi.x, b.hi.y, b.hi.z};
+    for (; g < groups; g += stride) {
+        const float4 a0 = __ldcs(q + 3 * g), b0 = __ldcs(q + 3 * g + 1), c0 = __ldcs(q + 3 * g + 2);
+        ext(0, a0.x); ext(1, a0.y); ext(2, a0.z); ext(0, a0.w); ext(1, b0.x); ext(2, b0.y);
+        ext(0, b0.z); ext(1, b0.w); ext(2, c0.x); ext(0, c0.y); ext(1, c0.z); ext(2, c0.w);
+    }
+    for (uint64_t i = groups * 12 + (uint64_t)blockIdx.x * kBlock + threadIdx.x; i < nf; i += stride)
+        ext((int)(i % 3), __ldg(f + i));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
-        for (int c = 0; c < 3; c++) v[c] = fminf(v[c], __shfl_xor_sync(0xFFFFFFFFu, v[c], o));
-#pragma unroll
-        for (int c = 3; c < 6; c++) v[c] = fmaxf(v[c], __shfl_xor_sync(0xFFFFFFFFu, v[c], o));
+        for (int c = 0; c < 3; c++) {
+            lo[c] = fminf(lo[c], __shfl_xor_sync(0xFFFFFFFFu, lo[c], o));
+            hi[c] = fmaxf(hi[c], __shfl_xor_sync(0xFFFFFFFFu, hi[c], o));
+        }
     }
-    if ((threadIdx.x & 31) == 0 && v[0] <= v[3]) {
-        for (int c = 0; c < 3; c++) atomicMax(&s->aabb_enc[c], ~ord(v[c]));
-        for (int c = 3; c < 6; c++) atomicMax(&s->aabb_enc[c], ord(v[c]));
+    __shared__ float red[kBlock / 32][6];
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0)
+        for (int c = 0; c < 3; c++) { red[w][c] = lo[c]; red[w][3 + c] = hi[c]; }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int c = threadIdx.x;
+        float v = red[0][c];
+        for (int k = 1; k < kBlock / 32; k++) v = c < 3 ? fminf(v, red[k][c]) : fmaxf(v, red[k][c]);
+        // blocks without data contribute +-FLT_MAX, which never wins
+        atomicMax(&s->aabb_enc[c], c < 3 ? ~ord(v) : ord(v));
     }
 }
 
@@ -161,6 +187,20 @@ __global__ void __launch_bounds__(kBlock) k_deltas(const unsigned long long* __r
     flags[i] = 0xFFFFFFFFu;
 }
 
+// Writes a finished node with four 16-byte stores (whole 32-byte sectors).
+PZ_D void store_node(Node* dst, const uint32_t c[2], const Box b[2], uint32_t parent, uint32_t context)
+{
+    float4* q = reinterpret_cast<float4*>(dst);
+    q[0] = make_float4(__uint_as_float(c[0]), __uint_as_float(c[1]), b[0].lo.x, b[0].lo.y);
+    q[1] = make_float4(b[0].lo.z, b[0].hi.x, b[0].hi.y, b[0].hi.z);
+    q[2] = make_float4(b[1].lo.x, b[1].lo.y, b[1].lo.z, b[1].hi.x);
+    q[3] = make_float4(b[1].hi.y, b[1].hi.z, __uint_as_float(parent), __uint_as_float(context));
+}
+
+// One thread per leaf climbs while it is the second to arrive at a node.  The first
+// arriver leaves its child index and box in the parent's slot; the exchange on the
+// handshake word is acquire-release, so the second arriver sees them.  A finished
+// node is kept in registers until its own parent is known and then written whole.
 __global__ void __launch_bounds__(kBlock) k_build(Node* __restrict__ nodes, uint32_t* __restrict__ rootOut,
                                                   const Tri* __restrict__ tris, uint32_t n,
                                                   const uint8_t* __restrict__ deltas, uint32_t* flags,
@@ -181,35 +221,41 @@ __global__ void __launch_bounds__(kBlock) k_build(Node* __restrict__ nodes, uint
     box_extend(box, mk3(__ldg(t + 0), __ldg(t + 1), __ldg(t + 2)));
     box_extend(box, mk3(__ldg(t + 3), __ldg(t + 4), __ldg(t + 5)));
     box_extend(box, mk3(__ldg(t + 6), __ldg(t + 7), __ldg(t + 8)));
+    bool pending = false;  // `node` is internal, finished, and not yet written
+    uint32_t pc[2], pctx = 0;
+    Box pb[2];
     bool isRoot = true;
     while (upper - lower < nInternals) {
-        uint32_t dL = 0 < lower ? __ldg(deltas + lower - 1) : 0xFFFFFFFFu;
-        uint32_t dR = upper < nInternals ? __ldg(deltas + upper) : 0xFFFFFFFFu;
-        int goLeft = dL < dR ? 1 : 0;
-        uint32_t parent = goLeft ? (lower - 1) : upper;
+        const uint32_t dL = 0 < lower ? __ldg(deltas + lower - 1) : 0xFFFFFFFFu;
+        const uint32_t dR = upper < nInternals ? __ldg(deltas + upper) : 0xFFFFFFFFu;
+        const int goLeft = dL < dR ? 1 : 0;
+        const uint32_t parent = goLeft ? (lower - 1) : upper;
+        if (pending) store_node(nodes + node_idx(node), pc, pb, make_node(parent, false), pctx);
+        pending = false;
         Node* P = nodes + parent;
         P->children[goLeft] = node;
         P->boxes[goLeft] = box;
-        if (!is_leaf(node)) nodes[node_idx(node)].parent = make_node(parent, false);
-        uint32_t other = goLeft ? upper : lower;
-        __threadfence();
-        other = atomicExch(flags + parent, other);
+        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> hs(flags[parent]);
+        const uint32_t other = hs.exchange(goLeft ? upper : lower, cuda::memory_order_acq_rel);
         if (other == 0xFFFFFFFFu) { isRoot = false; break; }
-        __threadfence();
         lower = min(lower, other);
         upper = max(upper, other);
-        P->context = upper < nInternals ? upper : 0xFFFFFFFFu;
-        node = make_node(parent, false);
-        // the sibling half was written by another thread: read it from L2
         const float* ob = reinterpret_cast<const float*>(&P->boxes[goLeft ^ 1]);
         Box o;
         o.lo = mk3(__ldcg(ob + 0), __ldcg(ob + 1), __ldcg(ob + 2));
         o.hi = mk3(__ldcg(ob + 3), __ldcg(ob + 4), __ldcg(ob + 5));
+        pc[goLeft] = node;
+        pc[goLeft ^ 1] = __ldcg(&P->children[goLeft ^ 1]);
+        pb[goLeft] = box;
+        pb[goLeft ^ 1] = o;
+        pctx = upper < nInternals ? upper : 0xFFFFFFFFu;
+        pending = true;
+        node = make_node(parent, false);
         box_extend(box, o);
     }
     if (isRoot) {
         *rootOut = node;
-        if (nInternals > 0) nodes[node_idx(node)].parent = kInvalidNode;
+        if (pending) store_node(nodes + node_idx(node), pc, pb, kInvalidNode, pctx);
     }
 }
 
@@ -253,7 +299,7 @@ cudaError_t build(const Tri* tris, uint32_t n, uint32_t opt, Node* nodes, uint32
         return cudaGetLastError();
     }
     const int grid = (int)min((uint32_t)(kNumSMs * 8), (n + kBlock - 1) / kBlock);
-    k_scene_aabb<<<grid, kBlock, 0, st>>>(tris, n, L.s);
+    k_scene_aabb<<<kNumSMs * 8, kBlock, 0, st>>>(tris, n, L.s);
     k_morton_hist<<<grid, kBlock, 0, st>>>(tris, n, opt, L.s, L.keys, L.lookback, (size_t)sort::num_tiles(n) * sort::kRadix);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (stopAfter == Stage::kKeys) return cudaSuccess;

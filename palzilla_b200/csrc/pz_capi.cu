@@ -110,9 +110,9 @@ extern "C" int pz_bvh_build(const pz_triangle* triangles_dev, int n, uint32_t bu
     if (scratch_bytes < bvh::scratch_bytes((uint32_t)n))
         return fail(PZ_ERR_SCRATCH_TOO_SMALL, "pz_bvh_build: scratch %zu < required %zu", scratch_bytes,
                     bvh::scratch_bytes((uint32_t)n));
-    if ((reinterpret_cast<uintptr_t>(triangles_dev) & 3) || (reinterpret_cast<uintptr_t>(internals_dev) & 3) ||
+    if ((reinterpret_cast<uintptr_t>(triangles_dev) & 3) || (reinterpret_cast<uintptr_t>(internals_dev) & 15) ||
         (reinterpret_cast<uintptr_t>(root_dev) & 3) || (reinterpret_cast<uintptr_t>(scratch_dev) & 255))
-        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_bvh_build: misaligned buffer (scratch needs 256-byte alignment)");
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_bvh_build: misaligned buffer (internals need 16-byte, scratch 256-byte alignment)");
     cudaError_t e = bvh::build(reinterpret_cast<const Tri*>(triangles_dev), (uint32_t)n, build_option,
                                reinterpret_cast<Node*>(internals_dev), root_dev, scratch_dev,
                                reinterpret_cast<cudaStream_t>(stream));

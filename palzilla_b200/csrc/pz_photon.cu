@@ -1,0 +1,146 @@
+// pz_photon.cu -- photon pass: trace photons from the point light through specular
+// triangles and gather the landing paths into the PathCache (photonTrace,
+// main_gpu.cu:56-211; PathCache::store, pk.h:291-349).
+//
+// Photon identity is (triangle, j): photon j of triangle t uses Sobol index j with
+// scramble seeds (iteration, t, 789) for the position and (iteration, t, 178) for
+// eta, and (j, depth, t, iteration) for the Fresnel choice at each bounce -- exactly
+// the reference's streams -- so the traced paths are bit-exact with the oracle (this
+// unit is compiled with -fmad=false).  One thread per photon: the grid covers
+// n_triangles x photons_per_triangle photons (the reference's 256-thread block per
+// triangle is the photons_per_triangle = 256 case).  Diffuse and back-facing
+// emitters retire at once, as in the reference.
+#include "pz_cache.cuh"
+#include "pz_optics.cuh"
+#include "pz_photon.cuh"
+#include "pz_trace.cuh"
+
+namespace pz {
+
+constexpr int kPhotonDepth = 4;  // PHOTON_TRACE_MAX_DEPTH, pk.h:33
+
+__global__ void __launch_bounds__(256) k_photon(const Node* __restrict__ nodes, const uint32_t* __restrict__ rootPtr,
+                                                const Tri* __restrict__ tris, const Attrib* __restrict__ attribs,
+                                                uint32_t nTris, uint32_t photonsPerTri, float3 p_light, float eta_min,
+                                                float eta_max, int iteration, float minThroughput, CacheView cache,
+                                                PhotonRecord* __restrict__ records)
+{
+    const uint64_t gid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t iTri = (uint32_t)(gid / photonsPerTri);
+    const uint32_t j = (uint32_t)(gid % photonsPerTri);
+    if (iTri >= nTris) return;
+    PhotonRecord rec;
+    rec.ev = 0;
+    bool emitted = false;
+    const uint32_t root = __ldg(rootPtr);
+
+    const int32_t mat0 = __ldg(&attribs[iTri].material);
+    if (mat0 != kDiffuse) {
+        float3 v0, v1, v2;
+        load_tri(tris, iTri, v0, v1, v2);
+        float3 ng0 = cross(v1 - v0, v2 - v0);
+        const float* an = reinterpret_cast<const float*>(attribs + iTri) + 1;
+        float3 ns0 = mk3(__ldg(an + 0), __ldg(an + 1), __ldg(an + 2));
+        ng0 = ng0 * dot(ng0, ns0);
+        if (!(dot(ng0, p_light - v0) < 0.0f)) {
+            float2 prm;
+            sobol2d(&prm.x, &prm.y, j, (uint32_t)iteration, iTri, 789u);
+            prm = square2triangle(prm);
+            float2 er;
+            sobol2d(&er.x, &er.y, j, (uint32_t)iteration, iTri, 178u);
+            const float eta = lerpf(eta_min, eta_max, er.x);
+            const float3 p = v0 + (v1 - v0) * prm.x + (v2 - v0) * prm.y;
+            float3 ro = p_light, rd = p - p_light;
+            uint32_t ev = 0;
+            int K = 0;
+            bool admissible = false;
+            float throughput = 1.0f;
+            float3 p_final = mk3(0.f, 0.f, 0.f);
+            int triIdx[kPhotonDepth] = {0, 0, 0, 0};
+            float params[2 * kPhotonDepth] = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (int d = 0; d < kPhotonDepth + 1; d++) {
+                Hit hit = make_miss();
+                closest_hit(hit, nodes, tris, root, ro, rd, &cache.h->status);
+                if (hit.t == kFltMax) break;
+                const Attrib* A = attribs + hit.tri;
+                const int32_t m = __ldg(&A->material);
+                const float* sn = reinterpret_cast<const float*>(A) + 1;
+                const float3 n0 = mk3(__ldg(sn + 0), __ldg(sn + 1), __ldg(sn + 2));
+                const float3 n1 = mk3(__ldg(sn + 3), __ldg(sn + 4), __ldg(sn + 5));
+                const float3 n2 = mk3(__ldg(sn + 6), __ldg(sn + 7), __ldg(sn + 8));
+                const float3 p_hit = ro + rd * hit.t;
+                const float3 ns = n0 + (n1 - n0) * hit.u + (n2 - n0) * hit.v;
+                if (m == kDiffuse) {
+                    if (d == 0) break;
+                    admissible = true;
+                    p_final = p_hit;
+                    break;
+                }
+                if (d == kPhotonDepth) break;
+                const float3 wi = -rd;
+                triIdx[d] = (int)hit.tri;
+                params[2 * d] = hit.u;
+                params[2 * d + 1] = hit.v;
+                float2 rnd;
+                sobol2d(&rnd.x, &rnd.y, j, (uint32_t)d, iTri, (uint32_t)iteration);
+                const float reflectance = fresnel_exact_norm_free(wi, ns, eta);
+                const bool isT = (m == kDielectric) && !(rnd.x < reflectance);
+                if (isT) ev |= 1u << K;
+                K++;
+                float sign = 1.0f;
+                float3 wo;
+                if (!isT) {
+                    wo = reflection(wi, ns);
+                    if (m == kDielectric) throughput *= reflectance;
+                } else {
+                    if (!refraction_norm_free(&wo, wi, ns, eta)) break;
+                    sign = -1.0f;
+                    throughput *= 1.0f - reflectance;
+                }
+                if (0.0f < dot(hit.ng, wi) * dot(hit.ng, wo) * sign) {
+                    const float3 od = normalize(hit.ng * dot(hit.ng, wo));
+                    ro = p_hit + od * ray_offset_scale(p_hit);
+                    rd = wo;
+                    continue;
+                }
+                break;
+            }
+            if (admissible && minThroughput < throughput) {
+                ev |= (uint32_t)K << 24;
+                emitted = true;
+                if (cache.hash) cache_store(cache, p_final, triIdx, params, ev);
+                if (records) {
+                    rec.ev = ev;
+                    for (int d = 0; d < 4; d++) rec.tris[d] = triIdx[d];
+                    for (int d = 0; d < 8; d++) rec.params[d] = params[d];
+                    rec.p[0] = p_final.x;
+                    rec.p[1] = p_final.y;
+                    rec.p[2] = p_final.z;
+                }
+            }
+        }
+    }
+    if (records) {
+        if (!emitted) {
+            for (int d = 0; d < 4; d++) rec.tris[d] = 0;
+            for (int d = 0; d < 8; d++) rec.params[d] = 0.0f;
+            rec.p[0] = rec.p[1] = rec.p[2] = 0.0f;
+        }
+        records[gid] = rec;
+    }
+}
+
+cudaError_t launch_photons(const Node* nodes, const uint32_t* root, const Tri* tris, const Attrib* attribs,
+                           uint32_t nTris, uint32_t photonsPerTri, float3 p_light, float eta_min, float eta_max,
+                           int iteration, float minThroughput, const CacheView& cache, PhotonRecord* records,
+                           cudaStream_t s)
+{
+    const uint64_t total = (uint64_t)nTris * photonsPerTri;
+    if (total == 0) return cudaSuccess;
+    const uint64_t blocks = (total + 255) / 256;
+    k_photon<<<(unsigned)blocks, 256, 0, s>>>(nodes, root, tris, attribs, nTris, photonsPerTri, p_light, eta_min,
+                                              eta_max, iteration, minThroughput, cache, records);
+    return cudaGetLastError();
+}
+
+}  // namespace pz

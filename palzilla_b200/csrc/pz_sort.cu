@@ -79,42 +79,48 @@ PZ_D uint32_t block_exclusive_scan(uint32_t x, uint32_t* ws)
 
 template <class KeyT, bool kHasVal>
 struct PassSmem {
-    KeyT keys[kTile];
+    KeyT keys[kTile];                 // tile in digit order
     uint32_t vals[kHasVal ? kTile : 1];
-    uint16_t wcnt[kWarps][kRadix];   // per-warp digit counts, then per-warp exclusive offsets
-    uint32_t dstart[kRadix];         // tile-local exclusive digit start
-    uint32_t gbase[kRadix];          // global destination of the digit run minus dstart
+    uint32_t off[kWarps][kRadix];     // per-warp digit counts, then per-warp positions
+    uint32_t gbase[kRadix];           // global destination of the digit run minus its tile start
     uint32_t ws[2][kWarps];
     uint32_t tile;
 };
 
-template <class KeyT, bool kHasVal>
-__global__ void __launch_bounds__(kThreads) k_pass(const KeyT* __restrict__ kin, KeyT* __restrict__ kout,
-                                                   const uint32_t* __restrict__ vin, uint32_t* __restrict__ vout,
-                                                   uint32_t n, int bit, int pass, Header* __restrict__ h,
-                                                   unsigned long long* __restrict__ lookback)
+// Peers of this lane: the valid lanes of the warp holding the same digit.
+template <bool kAllValid>
+PZ_D uint32_t digit_peers(uint32_t d, bool valid)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    auto& S = *reinterpret_cast<PassSmem<KeyT, kHasVal>*>(smem_raw);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-
-    if (tid == 0) S.tile = atomicAdd(&h->tile_counter[pass], 1u);
-    {
-        uint32_t* wc = reinterpret_cast<uint32_t*>(&S.wcnt[0][0]);
-        for (int i = tid; i < kWarps * kRadix / 2; i += kThreads) wc[i] = 0;
+    const uint32_t vmask = kAllValid ? 0xFFFFFFFFu : __ballot_sync(0xFFFFFFFFu, valid);
+    if (kRankMatch) return __match_any_sync(0xFFFFFFFFu, valid ? d : 0x100u) & vmask;
+    uint32_t peers = vmask;
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+        const bool set = (d >> b) & 1u;
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, set);
+        peers &= set ? bal : ~bal;
     }
-    __syncthreads();
-    const uint32_t tile = S.tile;
+    return peers;
+}
+
+// One tile of a digit pass; kFull = the tile has kTile items (no per-item bounds checks).
+template <class KeyT, bool kHasVal, bool kFull>
+PZ_D void pass_tile(PassSmem<KeyT, kHasVal>& S, const KeyT* __restrict__ kin, KeyT* __restrict__ kout,
+                    const uint32_t* __restrict__ vin, uint32_t* __restrict__ vout, uint32_t n, int bit, int pass,
+                    Header* __restrict__ h, unsigned long long* __restrict__ lookback, uint32_t tile)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t base = tile * kTile;
 
-    // ---- load (warp-striped: warp w owns items [w*512, w*512+512) of the tile)
+    // ---- load: warp w owns items [w * 32 * kItems, (w + 1) * 32 * kItems) of the tile,
+    //      item k of lane l at offset k * 32 + l (coalesced, and (k, lane) is input order)
     KeyT key[kItems];
     uint32_t val[kHasVal ? kItems : 1];
     const uint32_t wbase = base + warp * (kItems * 32);
 #pragma unroll
     for (int k = 0; k < kItems; k++) {
-        uint32_t idx = wbase + k * 32 + lane;
-        if (idx < n) {
+        const uint32_t idx = wbase + k * 32 + lane;
+        if (kFull || idx < n) {
             key[k] = __ldcs(kin + idx);
             if (kHasVal) val[k] = __ldcs(vin + idx);
         } else {
@@ -123,88 +129,109 @@ __global__ void __launch_bounds__(kThreads) k_pass(const KeyT* __restrict__ kin,
         }
     }
 
-    // ---- stable warp ranking, item order = (k, lane)
-    uint16_t rank[kItems];
+    // ---- per-warp digit counts: either counted up front (the tile aggregate can then be
+    //      published before ranking) or produced by the ranking itself
+    uint16_t rank[kEarlyCounts ? 1 : kItems];
     const uint32_t ltmask = (1u << lane) - 1u;
+    if (kEarlyCounts) {
 #pragma unroll
-    for (int k = 0; k < kItems; k++) {
-        const uint32_t idx = wbase + k * 32 + lane;
-        const bool valid = idx < n;
-        const uint32_t d = digit_of(key[k], bit);
-        uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);
-#pragma unroll
-        for (int b = 0; b < 8; b++) {
-            const bool set = (d >> b) & 1u;
-            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, set);
-            peers &= set ? bal : ~bal;
-        }
-        const uint32_t before = __popc(peers & ltmask);
-        const uint32_t cnt = valid ? S.wcnt[warp][d] : 0u;
-        __syncwarp();
-        if (valid && before == 0) S.wcnt[warp][d] = (uint16_t)(cnt + __popc(peers));
-        __syncwarp();
-        rank[k] = (uint16_t)(cnt + before);
-    }
-    __syncthreads();
-
-    // ---- per digit (thread = digit): warp offsets, tile total, tile-local start
-    const int d = tid;
-    uint32_t total = 0;
-#pragma unroll
-    for (int w = 0; w < kWarps; w++) {
-        uint32_t c = S.wcnt[w][d];
-        S.wcnt[w][d] = (uint16_t)total;
-        total += c;
-    }
-    const uint32_t gcount = h->hist[pass][d];
-    const uint32_t dstart = block_exclusive_scan(total, S.ws[0]);
-    const uint32_t gexcl = block_exclusive_scan(gcount, S.ws[1]);
-    S.dstart[d] = dstart;
-
-    // ---- decoupled look-back over earlier tiles for digit d
-    const unsigned long long tag = (unsigned long long)(pass + 1) << 34;
-    unsigned long long* mine = lookback + (size_t)tile * kRadix + d;
-    uint32_t prefix = 0;
-    if (tile == 0) {
-        st_volatile(mine, tag | kFlagP | total);
+        for (int k = 0; k < kItems; k++)
+            if (kFull || wbase + k * 32 + lane < n) atomicAdd(&S.off[warp][digit_of(key[k], bit)], 1u);
     } else {
-        st_volatile(mine, tag | kFlagA | total);
-        int t = (int)tile - 1;
-        uint32_t spins = 0;
-        while (t >= 0) {
-            unsigned long long w = ld_volatile(lookback + (size_t)t * kRadix + d);
-            if ((w & ~0x3FFFFFFFFull) != tag || (w & (3ull << 32)) == 0) {
-                if (++spins > kSpinLimit) {
-                    raise_error(&h->status, kErrSpinLimit);
-                    break;
-                }
-                if (spins > 64) __nanosleep(64);
-                continue;
-            }
-            prefix += (uint32_t)w;
-            if (w & kFlagP) break;
-            t--;
+#pragma unroll
+        for (int k = 0; k < kItems; k++) {
+            const bool valid = kFull || wbase + k * 32 + lane < n;
+            const uint32_t dd = digit_of(key[k], bit);
+            const uint32_t peers = digit_peers<kFull>(dd, valid);
+            const uint32_t before = __popc(peers & ltmask);
+            const uint32_t cnt = valid ? S.off[warp][dd] : 0u;
+            __syncwarp();
+            if (valid && before == 0) S.off[warp][dd] = cnt + __popc(peers);
+            __syncwarp();
+            rank[k] = (uint16_t)(cnt + before);
         }
-        st_volatile(mine, tag | kFlagP | (uint32_t)(prefix + total));
     }
-    S.gbase[d] = gexcl + prefix - dstart;
     __syncthreads();
 
-    // ---- scatter into shared memory in digit order
+    // ---- per digit (thread = digit, kThreads >= kRadix): per-warp positions, tile
+    //      total, aggregate published for later tiles
+    const int d = tid;
+    uint32_t total = 0, dstart = 0, gexcl = 0;
+    uint32_t wc[kWarps];
+    const unsigned long long tag = (unsigned long long)(pass + 1) << 34;
+    unsigned long long* mine = lookback + (size_t)tile * kRadix + (d < kRadix ? d : 0);
+    if (d < kRadix) {
+#pragma unroll
+        for (int w = 0; w < kWarps; w++) {
+            wc[w] = S.off[w][d];
+            total += wc[w];
+        }
+        st_volatile(mine, tag | (tile == 0 ? kFlagP : kFlagA) | total);
+    }
+    const uint32_t gcount = d < kRadix ? h->hist[pass][d] : 0u;
+    dstart = block_exclusive_scan(total, S.ws[0]);
+    gexcl = block_exclusive_scan(gcount, S.ws[1]);
+    if (d < kRadix) {
+        uint32_t run = dstart;
+#pragma unroll
+        for (int w = 0; w < kWarps; w++) {
+            S.off[w][d] = run;
+            run += wc[w];
+        }
+    }
+    __syncthreads();
+
+    // ---- place every key at its tile position in shared memory (digit order, stable)
 #pragma unroll
     for (int k = 0; k < kItems; k++) {
-        const uint32_t idx = wbase + k * 32 + lane;
-        if (idx < n) {
-            const uint32_t dd = digit_of(key[k], bit);
-            const uint32_t pos = S.dstart[dd] + S.wcnt[warp][dd] + rank[k];
+        const bool valid = kFull || wbase + k * 32 + lane < n;
+        const uint32_t dd = digit_of(key[k], bit);
+        if (kEarlyCounts) {
+            const uint32_t peers = digit_peers<kFull>(dd, valid);
+            const uint32_t before = __popc(peers & ltmask);
+            const uint32_t run = valid ? S.off[warp][dd] : 0u;
+            __syncwarp();
+            if (valid) {
+                S.keys[run + before] = key[k];
+                if (kHasVal) S.vals[run + before] = val[k];
+                if (before == 0) S.off[warp][dd] = run + __popc(peers);
+            }
+            __syncwarp();
+        } else if (valid) {
+            const uint32_t pos = S.off[warp][dd] + rank[k];
             S.keys[pos] = key[k];
             if (kHasVal) S.vals[pos] = val[k];
         }
     }
+
+    // ---- decoupled look-back over earlier tiles for digit d
+    if (d < kRadix) {
+        uint32_t prefix = 0;
+        if (tile != 0) {
+            int t = (int)tile - 1;
+            uint32_t spins = 0;
+            while (t >= 0) {
+                const unsigned long long w = ld_volatile(lookback + (size_t)t * kRadix + d);
+                if ((w & ~0x3FFFFFFFFull) != tag || (w & (3ull << 32)) == 0) {
+                    if (++spins > kSpinLimit) {
+                        raise_error(&h->status, kErrSpinLimit);
+                        break;
+                    }
+                    if (spins > 16) __nanosleep(32);
+                    continue;
+                }
+                prefix += (uint32_t)w;
+                if (w & kFlagP) break;
+                t--;
+            }
+            st_volatile(mine, tag | kFlagP | (uint32_t)(prefix + total));
+        }
+        S.gbase[d] = gexcl + prefix - dstart;
+    }
     __syncthreads();
 
     // ---- write digit runs to their global positions
-    const uint32_t tileN = min((uint32_t)kTile, n - base);
+    const uint32_t tileN = kFull ? (uint32_t)kTile : min((uint32_t)kTile, n - base);
 #pragma unroll 4
     for (uint32_t i = tid; i < tileN; i += kThreads) {
         const KeyT kk = S.keys[i];
@@ -214,6 +241,25 @@ __global__ void __launch_bounds__(kThreads) k_pass(const KeyT* __restrict__ kin,
             if (kHasVal) vout[dst] = S.vals[i];
         }
     }
+}
+
+template <class KeyT, bool kHasVal>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass(const KeyT* __restrict__ kin, KeyT* __restrict__ kout,
+                                                               const uint32_t* __restrict__ vin,
+                                                               uint32_t* __restrict__ vout, uint32_t n, int bit,
+                                                               int pass, Header* __restrict__ h,
+                                                               unsigned long long* __restrict__ lookback)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto& S = *reinterpret_cast<PassSmem<KeyT, kHasVal>*>(smem_raw);
+    if (threadIdx.x == 0) S.tile = atomicAdd(&h->tile_counter[pass], 1u);
+    for (int i = threadIdx.x; i < kWarps * kRadix; i += kThreads) (&S.off[0][0])[i] = 0;
+    __syncthreads();
+    const uint32_t tile = S.tile;
+    if ((uint64_t)(tile + 1) * kTile <= n)
+        pass_tile<KeyT, kHasVal, true>(S, kin, kout, vin, vout, n, bit, pass, h, lookback, tile);
+    else
+        pass_tile<KeyT, kHasVal, false>(S, kin, kout, vin, vout, n, bit, pass, h, lookback, tile);
 }
 
 // ---------------------------------------------------------------------------

@@ -23,10 +23,31 @@
 namespace pz {
 namespace sort {
 
-constexpr int kThreads = 256;
+// Compile-time shape of the digit pass (chosen by the sweep recorded in profiles/):
+// threads per tile, items per thread, ranking by warp ballots (0) or match.any (1),
+// digit counts before ranking (1) or from the ranking (0).
+#ifndef PZ_SORT_THREADS
+#define PZ_SORT_THREADS 256
+#endif
+#ifndef PZ_SORT_ITEMS
+#define PZ_SORT_ITEMS 16
+#endif
+#ifndef PZ_SORT_RANK_MATCH
+#define PZ_SORT_RANK_MATCH 0
+#endif
+#ifndef PZ_SORT_EARLY_COUNTS
+#define PZ_SORT_EARLY_COUNTS 1
+#endif
+#ifndef PZ_SORT_MIN_BLOCKS
+#define PZ_SORT_MIN_BLOCKS 4
+#endif
+constexpr int kThreads = PZ_SORT_THREADS;
 constexpr int kWarps = kThreads / 32;
-constexpr int kItems = 16;
-constexpr int kTile = kThreads * kItems;  // 4096 items per tile
+constexpr int kItems = PZ_SORT_ITEMS;
+constexpr bool kRankMatch = PZ_SORT_RANK_MATCH != 0;
+constexpr bool kEarlyCounts = PZ_SORT_EARLY_COUNTS != 0;
+constexpr int kMinBlocks = PZ_SORT_MIN_BLOCKS;
+constexpr int kTile = kThreads * kItems;  // items per tile
 constexpr int kRadix = 256;
 constexpr int kMaxPasses = 8;
 constexpr int kHistBlocksPerSM = 4;

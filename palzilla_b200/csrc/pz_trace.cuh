@@ -1,0 +1,178 @@
+// pz_trace.cuh -- BVH traversal on the InternalNode layout.
+//
+// closest_hit: near-first stackful traversal (intersect_stackfull, minimum_lbvh.h:927-988).
+// any_hit:     stackless escape-link traversal (intersect_escape_link with RAY_QUERY_ANY,
+//              minimum_lbvh.h:1078-1152), used for occlusion.
+// Both visit nodes in the reference's order, so ties between equal-t hits resolve to
+// the same triangle and any-hit queries stop on the same first hit.  Nodes are read
+// as four 16-byte loads through the read-only path; the closest-hit stack lives in
+// registers / local memory (kStack entries) instead of the reference's global
+// per-warp stack pool (pk.h:1113-1168), and overflow is reported, not silently
+// corrupted.
+#pragma once
+#include "pz_common.cuh"
+
+namespace pz {
+
+struct Hit {
+    float t;
+    float u, v;
+    float3 ng;
+    uint32_t tri;
+};
+
+struct NodeView {
+    uint32_t c0, c1;
+    float3 lo0, hi0, lo1, hi1;
+    uint32_t parent, context;
+};
+
+PZ_D NodeView load_node(const Node* nodes, uint32_t i)
+{
+    const float4* p = reinterpret_cast<const float4*>(nodes + i);
+    float4 a = __ldg(p + 0), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
+    NodeView n;
+    n.c0 = __float_as_uint(a.x);
+    n.c1 = __float_as_uint(a.y);
+    n.lo0 = mk3(a.z, a.w, b.x);
+    n.hi0 = mk3(b.y, b.z, b.w);
+    n.lo1 = mk3(c.x, c.y, c.z);
+    n.hi1 = mk3(c.w, d.x, d.y);
+    n.parent = __float_as_uint(d.z);
+    n.context = __float_as_uint(d.w);
+    return n;
+}
+
+PZ_D void load_tri(const Tri* tris, uint32_t i, float3& v0, float3& v1, float3& v2)
+{
+    const float* t = reinterpret_cast<const float*>(tris) + (size_t)i * 9;
+    v0 = mk3(__ldg(t + 0), __ldg(t + 1), __ldg(t + 2));
+    v1 = mk3(__ldg(t + 3), __ldg(t + 4), __ldg(t + 5));
+    v2 = mk3(__ldg(t + 6), __ldg(t + 7), __ldg(t + 8));
+}
+
+constexpr int kStack = 64;
+
+PZ_D void closest_hit(Hit& hit, const Node* __restrict__ nodes, const Tri* __restrict__ tris, uint32_t root, float3 ro,
+                      float3 rd, uint32_t* status)
+{
+    const float3 inv = inv_rd(rd);
+    uint32_t stack[kStack];
+    int sp = 0;
+    uint32_t node = root;
+    while (node != kInvalidNode) {
+        if (is_leaf(node)) {
+            float3 v0, v1, v2;
+            load_tri(tris, node_idx(node), v0, v1, v2);
+            float t, u, v;
+            float3 ng;
+            if (ray_triangle(&t, &u, &v, &ng, 0.0f, hit.t, ro, rd, v0, v1, v2)) {
+                hit.t = t;
+                hit.u = u;
+                hit.v = v;
+                hit.ng = ng;
+                hit.tri = node_idx(node);
+            }
+            node = sp == 0 ? kInvalidNode : stack[--sp];
+            continue;
+        }
+        const NodeView n = load_node(nodes, node_idx(node));
+        float rl, rr;
+        const bool hl = slab_hit(ro, inv, n.lo0, n.hi0, hit.t, &rl);
+        const bool hr = slab_hit(ro, inv, n.lo1, n.hi1, hit.t, &rr);
+        if (hl && hr) {
+            uint32_t nearN = n.c0, farN = n.c1;
+            if (rr < rl) { nearN = n.c1; farN = n.c0; }
+            if (sp < kStack) stack[sp++] = farN;
+            else raise_error(status, kErrStackOverflow);
+            node = nearN;
+        } else if (hl || hr) {
+            node = hl ? n.c0 : n.c1;
+        } else {
+            node = sp == 0 ? kInvalidNode : stack[--sp];
+        }
+    }
+}
+
+PZ_D Hit make_miss()
+{
+    Hit h;
+    h.t = kFltMax;
+    h.u = h.v = 0.0f;
+    h.ng = mk3(0.f, 0.f, 0.f);
+    h.tri = 0xFFFFFFFFu;
+    return h;
+}
+
+// Escape-link any-hit query: returns the t of the first hit found (or tmax when none).
+PZ_D float any_hit(const Node* __restrict__ nodes, const Tri* __restrict__ tris, uint32_t root, float3 ro, float3 rd,
+                   float tmax)
+{
+    const float3 inv = inv_rd(rd);
+    float best = tmax;
+    uint32_t curr = root, prev = kInvalidNode;
+    while (curr != kInvalidNode) {
+        if (is_leaf(curr)) {
+            float3 v0, v1, v2;
+            load_tri(tris, node_idx(curr), v0, v1, v2);
+            float t, u, v;
+            float3 ng;
+            if (ray_triangle(&t, &u, &v, &ng, 0.0f, best, ro, rd, v0, v1, v2)) {
+                best = t;
+                break;
+            }
+            const NodeView p = load_node(nodes, node_idx(prev));
+            if (p.c0 == curr) {  // just go to the sibling side of prev
+                const uint32_t tmp = curr;
+                curr = prev;
+                prev = tmp;
+                continue;
+            }
+            const uint32_t next = p.context != 0xFFFFFFFFu ? make_node(p.context, false) : kInvalidNode;
+            prev = curr;
+            curr = next;
+            continue;
+        }
+        const NodeView n = load_node(nodes, node_idx(curr));
+        float3 lo, hi;
+        uint32_t hitChild, miss;
+        if (prev == n.parent) {
+            lo = n.lo0;
+            hi = n.hi0;
+            hitChild = n.c0;
+            miss = curr;
+        } else {
+            lo = n.lo1;
+            hi = n.hi1;
+            hitChild = n.c1;
+            miss = n.context != 0xFFFFFFFFu ? make_node(n.context, false) : kInvalidNode;
+        }
+        float rmin;
+        const uint32_t next = slab_hit(ro, inv, lo, hi, best, &rmin) ? hitChild : miss;
+        prev = curr;
+        curr = next;
+    }
+    return best;
+}
+
+// rayOffsetScale, pk.h:43-49
+PZ_D float ray_offset_scale(float3 p)
+{
+    p = vabs(p);
+    float m = fmaxf(fmaxf(fmaxf(p.x, p.y), p.z), 1.0f);
+    return m * 1.192092896e-07F * 128.0f;
+}
+
+// occluded, pk.h:88-115
+PZ_D bool occluded(const Node* nodes, const Tri* tris, uint32_t root, float3 from, float3 from_n, float3 to,
+                   float3 to_n)
+{
+    if (ex::dot(ex::sub3(to, from), from_n) < 0.0f) from_n = -from_n;
+    if (ex::dot(ex::sub3(from, to), to_n) < 0.0f) to_n = -to_n;
+    float3 from_safe = ex::add3(from, ex::mul3(from_n, ray_offset_scale(from)));
+    float3 to_safe = ex::add3(to, ex::mul3(to_n, ray_offset_scale(to)));
+    float3 rd = ex::sub3(to_safe, from_safe);
+    return any_hit(nodes, tris, root, from_safe, rd, 1.0f) < 1.0f;
+}
+
+}  // namespace pz
