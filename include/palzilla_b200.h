@@ -104,6 +104,120 @@ PZ_API int pz_bvh_build(const pz_triangle* triangles_dev, int n_triangles, uint3
 PZ_API int pz_bvh_debug_views(void* scratch_dev, int n_triangles, const uint64_t** sorted_dev, const uint8_t** deltas_dev,
                        pz_aabb* aabb_out, pz_stream_t stream);
 
+
+/* ---------------------------------------------------------------- ray queries
+ * Batch closest-hit (intersect_stackfull, minimum_lbvh.h:927-988) and any-hit
+ * (intersect_escape_link with RAY_QUERY_ANY, minimum_lbvh.h:1078-1152) queries.  Rays
+ * are 3 floats per ray (origin, direction); hit outputs may be NULL except t_dev.  A
+ * closest-hit miss reports t = FLT_MAX and triangle 0xFFFFFFFF; any-hit writes 1 when a
+ * hit with t < tmax exists. */
+PZ_API int pz_trace_closest(const pz_internal_node* internals_dev, const uint32_t* root_dev,
+                            const pz_triangle* triangles_dev, int n_rays, const float* ro_dev, const float* rd_dev,
+                            float* t_dev, float* uv_dev, uint32_t* tri_dev, float* ng_dev, uint32_t* status_dev,
+                            pz_stream_t stream);
+PZ_API int pz_trace_any(const pz_internal_node* internals_dev, const uint32_t* root_dev,
+                        const pz_triangle* triangles_dev, int n_rays, const float* ro_dev, const float* rd_dev,
+                        const float* tmax_dev, uint8_t* hit_dev, pz_stream_t stream);
+
+/* ---------------------------------------------------------------- PathCache
+ * Spatial hash of photon tuples (PathCache, pk.h:227-402) in one caller-owned buffer of
+ * pz_path_cache_bytes(capacity) bytes; capacity must be a power of two (the reference
+ * uses 2^22).  The status word (first 4 bytes) reports probe overflow. */
+PZ_API size_t pz_path_cache_bytes(uint32_t capacity);
+/* PathCache::clear (pk.h:254-269): empties the table and the counters. */
+PZ_API int pz_path_cache_clear(void* cache_dev, uint32_t capacity, pz_stream_t stream);
+/* Device addresses of the cache arrays (hash, cell hash, event descriptor, 4 triangle
+ * indices and 8 barycentrics per slot, stored-entry count). */
+PZ_API int pz_path_cache_views(void* cache_dev, uint32_t capacity, uint32_t** hash_dev, uint32_t** cell_dev,
+                               uint32_t** events_dev, int32_t** tris_dev, float** params_dev, uint32_t** count_dev);
+
+/* ---------------------------------------------------------------- photon pass
+ * photonTrace (main_gpu.cu:56-211): photons_per_triangle photons from every specular,
+ * light-facing triangle (the reference's 256-thread block per triangle is 256), up to 4
+ * Fresnel-sampled specular events to a diffuse landing, stored into the PathCache.
+ * records_dev (n_triangles * photons_per_triangle records, or NULL) receives every
+ * photon's path for inspection (ev = 0 when the photon produced none). */
+typedef struct pz_photon_record { uint32_t ev; int32_t tris[4]; float params[8]; float p[3]; } pz_photon_record;
+PZ_API int pz_photon_trace(const pz_internal_node* internals_dev, const uint32_t* root_dev,
+                           const pz_triangle* triangles_dev, const pz_triangle_attrib* attribs_dev, int n_triangles,
+                           int photons_per_triangle, pz_float3 p_light, float eta_min, float eta_max, int iteration,
+                           float min_throughput, void* cache_dev, uint32_t cache_capacity, float cell_step,
+                           pz_photon_record* records_dev, pz_stream_t stream);
+
+/* ---------------------------------------------------------------- eye pass */
+typedef struct pz_ray_generator { pz_float3 origin, right, up; } pz_ray_generator; /* RayGenerator, camera.h:4-41 */
+typedef struct pz_lens_params { float distance, thickness, R; } pz_lens_params;   /* LensParams, pk.h:1035-1040 */
+typedef struct pz_first_diffuse { pz_float3 p, ng, R; float lambda; } pz_first_diffuse; /* FirstDiffuse, pk.h:80-86 */
+/* RayGenerator::lookat (camera.h:10-22), on the host. */
+PZ_API void pz_ray_generator_lookat(pz_ray_generator* gen, pz_float3 eye, pz_float3 center, pz_float3 up, float fovy,
+                                    int width, int height);
+/* solvePrimary (main_gpu.cu:213-371).  accum_dev: 4 floats per pixel (RGB + sample
+ * count), added to.  The receiver albedo is a constant; lens->R <= 0 disables the lens. */
+PZ_API int pz_solve_primary(float* accum_dev, pz_first_diffuse* first_diffuse_dev, int width, int height,
+                            const pz_ray_generator* gen, const pz_lens_params* lens,
+                            const pz_internal_node* internals_dev, const uint32_t* root_dev,
+                            const pz_triangle* triangles_dev, const pz_triangle_attrib* attribs_dev, pz_float3 p_light,
+                            float light_intensity, float radiance_clamp, float cauchy_a, float cauchy_b,
+                            pz_float3 albedo, int iteration, uint32_t* status_dev, pz_stream_t stream);
+
+/* ---------------------------------------------------------------- (pixel, tuple) work list */
+typedef struct pz_specular_path { int32_t pixel; int32_t cache_index; } pz_specular_path; /* pk.h:1102-1106 */
+/* lookupFlatten (main_gpu.cu:373-416): appends {pixel, slot} and {path hash, index}
+ * (IndexedSpecularPath as u64: hash in bits 0..31) for every slot of each pixel's cell
+ * with the given event descriptor; *counter_dev (device) is the running count and must
+ * be zeroed by the caller.  Pixels whose entries would pass `capacity` are dropped and
+ * flagged in the cache status word. */
+PZ_API int pz_lookup_flatten(uint32_t events, pz_specular_path* paths_dev, uint64_t* indexed_dev,
+                             uint32_t* counter_dev, uint32_t capacity, const pz_first_diffuse* first_diffuse_dev,
+                             int n_pixels, void* cache_dev, uint32_t cache_capacity, float cell_step,
+                             pz_stream_t stream);
+/* reorderSpecularPath (main_gpu.cu:515-525): dst[i] = src[indexed[i] >> 32]. */
+PZ_API int pz_reorder_specular_paths(const uint64_t* indexed_dev, pz_specular_path* dst_dev,
+                                     const pz_specular_path* src_dev, uint32_t n, pz_stream_t stream);
+
+/* ---------------------------------------------------------------- specular solve
+ * Description of one specular solve over a work list (solveSpecularPath<K>,
+ * main_gpu.cu:418-486).  Reference mode (spectral == NULL): each item uses its pixel's
+ * sampled wavelength and adds RGB to accum (4 floats per pixel).  Binned mode
+ * (spectral != NULL): each (item, bin) uses etas[bin] and adds the clamped contribution
+ * to spectral[pixel * n_bins + bin]. */
+typedef struct pz_solve_desc {
+    int K;                                 /* chain length, 1..4 */
+    uint32_t events;                       /* EventDescriptor::asU32 (pk.h:156-158) */
+    const pz_specular_path* paths;         /* device work list */
+    uint64_t n_paths;
+    const pz_first_diffuse* first_diffuse; /* device, per pixel */
+    const pz_internal_node* internals;
+    const uint32_t* root;
+    const pz_triangle* triangles;
+    const pz_triangle_attrib* attribs;
+    void* cache;
+    uint32_t cache_capacity;
+    float cell_step;
+    pz_float3 p_light;
+    float light_intensity;                 /* 16 in the reference (pk.h:1686) */
+    float radiance_clamp;                  /* 12 (pk.h:1688) */
+    float cauchy_a, cauchy_b;              /* eta(lambda) = a + b / lambda^2, lambda in nm */
+    float* accum;
+    float* spectral;
+    const float* etas;                     /* device, n_bins */
+    int n_bins;
+    int max_iterations;                    /* 32 (main_gpu.cu:456) */
+    float cost_tolerance;                  /* 1e-10 */
+    int early_term_warmup;                 /* 1 */
+    unsigned long long* stats;             /* device u64[3]: items solved, converged, contributing (or NULL) */
+} pz_solve_desc;
+/* One thread per work item, one launch per call: the reference's plain structure. */
+PZ_API int pz_solve_specular_plain(const pz_solve_desc* desc, pz_stream_t stream);
+
+/* ---------------------------------------------------------------- resolve
+ * pack (main_gpu.cu:499-513): accumulator / count -> sRGB OETF -> RGBA8. */
+PZ_API int pz_resolve(uint32_t* pixels_dev, const float* accum_dev, int n_pixels, pz_stream_t stream);
+/* Spectral image -> linear sRGB (rgb_dev, 4 floats per pixel, may be NULL) and RGBA8
+ * (pixels_dev, may be NULL): (albedo/pi) * sum_b S_b * srgb(lambda_b) * dlambda. */
+PZ_API int pz_resolve_spectral(float* rgb_dev, uint32_t* pixels_dev, const float* spectral_dev, int n_pixels,
+                               int n_bins, float lambda_min, float lambda_max, pz_float3 albedo, pz_stream_t stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

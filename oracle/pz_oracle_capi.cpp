@@ -261,7 +261,7 @@ void pzo_solve_primary(float* accum, float* firstDiffuse, int W, int H, const fl
                 sph_intersect(&t1, &t1b, ro, rd, c1, R);
                 if (!(t1 < 0.0f)) {
                     F3 hit1 = ro + rd * t1;
-                    F3 wo;
+                    F3 wo = rd;
                     refraction_norm_free(&wo, -rd, hit1 - c1, eta);
                     rd = wo;
                     ro = hit1;

@@ -22,6 +22,31 @@ sz = C.c_size_t
 i64 = C.c_int64
 u64 = C.c_uint64
 
+class Float3(C.Structure):
+    _fields_ = [("x", f32), ("y", f32), ("z", f32)]
+
+
+class RayGenerator(C.Structure):
+    _fields_ = [("origin", Float3), ("right", Float3), ("up", Float3)]
+
+
+class LensParams(C.Structure):
+    _fields_ = [("distance", f32), ("thickness", f32), ("R", f32)]
+
+
+class SolveDesc(C.Structure):
+    _fields_ = [("K", i32), ("events", u32), ("paths", vp), ("n_paths", u64), ("first_diffuse", vp),
+                ("internals", vp), ("root", vp), ("triangles", vp), ("attribs", vp), ("cache", vp),
+                ("cache_capacity", u32), ("cell_step", f32), ("p_light", Float3), ("light_intensity", f32),
+                ("radiance_clamp", f32), ("cauchy_a", f32), ("cauchy_b", f32), ("accum", vp), ("spectral", vp),
+                ("etas", vp), ("n_bins", i32), ("max_iterations", i32), ("cost_tolerance", f32),
+                ("early_term_warmup", i32), ("stats", vp)]
+
+
+def f3(v) -> Float3:
+    return Float3(float(v[0]), float(v[1]), float(v[2]))
+
+
 # name -> (restype, argtypes); mirrors include/palzilla_b200.h
 SIGNATURES = {
     "pz_version": (i32, []),
@@ -32,6 +57,21 @@ SIGNATURES = {
     "pz_bvh_scratch_bytes": (sz, [i32]),
     "pz_bvh_build": (i32, [vp, i32, u32, vp, vp, vp, sz, vp]),
     "pz_bvh_debug_views": (i32, [vp, i32, C.POINTER(vp), C.POINTER(vp), vp, vp]),
+    "pz_trace_closest": (i32, [vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "pz_trace_any": (i32, [vp, vp, vp, i32, vp, vp, vp, vp, vp]),
+    "pz_path_cache_bytes": (sz, [u32]),
+    "pz_path_cache_clear": (i32, [vp, u32, vp]),
+    "pz_path_cache_views": (i32, [vp, u32, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
+                                  C.POINTER(vp), C.POINTER(vp)]),
+    "pz_photon_trace": (i32, [vp, vp, vp, vp, i32, i32, Float3, f32, f32, i32, f32, vp, u32, f32, vp, vp]),
+    "pz_ray_generator_lookat": (None, [C.POINTER(RayGenerator), Float3, Float3, Float3, f32, i32, i32]),
+    "pz_solve_primary": (i32, [vp, vp, i32, i32, C.POINTER(RayGenerator), C.POINTER(LensParams), vp, vp, vp, vp,
+                               Float3, f32, f32, f32, f32, Float3, i32, vp, vp]),
+    "pz_lookup_flatten": (i32, [u32, vp, vp, vp, u32, vp, i32, vp, u32, f32, vp]),
+    "pz_reorder_specular_paths": (i32, [vp, vp, vp, u32, vp]),
+    "pz_solve_specular_plain": (i32, [C.POINTER(SolveDesc), vp]),
+    "pz_resolve": (i32, [vp, vp, i32, vp]),
+    "pz_resolve_spectral": (i32, [vp, vp, vp, i32, i32, f32, f32, Float3, vp]),
 }
 
 _lib = None
@@ -66,5 +106,6 @@ def check(code: int, where: str) -> None:
 
 def call(name: str, *args):
     r = getattr(lib(), name)(*args)
-    check(r, name)
+    if SIGNATURES[name][0] is i32:
+        check(r, name)
     return r

@@ -120,3 +120,184 @@ class BVHGPUBuilder:
         sorted_ = self.scratch.buf[so:so + 8 * n].view(torch.int64)
         deltas = self.scratch.buf[do:do + max(n - 1, 0)]
         return sorted_, deltas, list(aabb)
+
+
+# ---------------------------------------------------------------------------------------
+# photon pass, eye pass, work list, specular solve
+# ---------------------------------------------------------------------------------------
+def _vp(t):
+    return C.c_void_p(None if t is None else t.data_ptr())
+
+
+class DeviceScene:
+    """Device copies of a scene (triangles, attributes) and its LBVH."""
+
+    def __init__(self, scene, device="cuda", build_option: int = 0, stream=None):
+        import numpy as np
+        self.scene = scene
+        self.n = scene.n
+        self.tris = torch.from_numpy(np.ascontiguousarray(scene.tris)).to(device)
+        self.attribs = torch.from_numpy(np.ascontiguousarray(scene.attribs).view(np.uint8)).to(device)
+        self.builder = BVHGPUBuilder(device)
+        self.builder.build(self.tris, self.n, build_option, None, stream)
+
+    @property
+    def internals(self):
+        return self.builder.m_internals
+
+    @property
+    def root_dev(self):
+        return self.builder.m_rootNode
+
+
+class PathCache:
+    """PathCache (pk.h:227-402): one device buffer of pz_path_cache_bytes(capacity)."""
+
+    def __init__(self, capacity: int = 1 << 22, step: float = 0.01, device="cuda"):
+        self.capacity = capacity
+        self.step = step
+        self.buf = torch.empty(_lib.lib().pz_path_cache_bytes(capacity), dtype=torch.uint8, device=device)
+        self.clear()
+
+    def clear(self, stream=None):
+        _lib.call("pz_path_cache_clear", _vp(self.buf), C.c_uint32(self.capacity), C.c_void_p(_stream(stream)))
+
+    def views(self):
+        ptrs = [C.c_void_p() for _ in range(6)]
+        _lib.call("pz_path_cache_views", _vp(self.buf), C.c_uint32(self.capacity), *[C.byref(p) for p in ptrs])
+        base = self.buf.data_ptr()
+
+        def sl(p, nbytes):
+            o = p.value - base
+            return self.buf[o:o + nbytes]
+        cap = self.capacity
+        return dict(hash=sl(ptrs[0], 4 * cap).view(torch.int32), cell=sl(ptrs[1], 4 * cap).view(torch.int32),
+                    events=sl(ptrs[2], 4 * cap).view(torch.int32), tris=sl(ptrs[3], 16 * cap).view(torch.int32),
+                    params=sl(ptrs[4], 32 * cap).view(torch.float32), count=sl(ptrs[5], 4).view(torch.int32))
+
+    def to_host(self):
+        import numpy as np
+        v = self.views()
+        return dict(hash=v["hash"].cpu().numpy().view(np.uint32), cell=v["cell"].cpu().numpy().view(np.uint32),
+                    events=v["events"].cpu().numpy().view(np.uint32),
+                    tris=v["tris"].cpu().numpy().reshape(-1, 4), params=v["params"].cpu().numpy().reshape(-1, 8),
+                    count=int(v["count"].item()), capacity=self.capacity, step=self.step)
+
+    def status(self, stream=None) -> int:
+        st = C.c_uint32(0)
+        _lib.call("pz_scratch_status", _vp(self.buf), C.byref(st), C.c_void_p(_stream(stream)))
+        return st.value
+
+
+def photon_trace(ds: DeviceScene, cache: PathCache | None, iteration: int = 0, photons_per_triangle=None,
+                 eta_range=None, records: bool = False, stream=None):
+    """photonTrace (main_gpu.cu:56-211).  Returns the per-photon record tensor when asked."""
+    sc = ds.scene
+    ppt = photons_per_triangle or sc.photons_per_triangle
+    emin, emax = eta_range or sc.eta_range()
+    rec = torch.empty(ds.n * ppt * 64, dtype=torch.uint8, device=ds.tris.device) if records else None
+    _lib.call("pz_photon_trace", _vp(ds.internals), _vp(ds.root_dev), _vp(ds.tris), _vp(ds.attribs),
+              C.c_int(ds.n), C.c_int(ppt), _lib.f3(sc.p_light), C.c_float(emin), C.c_float(emax), C.c_int(iteration),
+              C.c_float(sc.min_throughput), _vp(cache.buf if cache else None),
+              C.c_uint32(cache.capacity if cache else 0), C.c_float(cache.step if cache else 0.0), _vp(rec),
+              C.c_void_p(_stream(stream)))
+    return rec
+
+
+def ray_generator(scene) -> "_lib.RayGenerator":
+    cam = scene.camera
+    g = _lib.RayGenerator()
+    _lib.lib().pz_ray_generator_lookat(C.byref(g), _lib.f3(cam.eye), _lib.f3(cam.center), _lib.f3(cam.up),
+                                       C.c_float(cam.fovy), C.c_int(scene.width), C.c_int(scene.height))
+    return g
+
+
+class Frame:
+    """Per-frame device buffers of the reference renderer (pk.h:1368-1391 subset)."""
+
+    def __init__(self, scene, path_capacity: int = 1 << 25, device="cuda"):
+        W, H = scene.width, scene.height
+        self.npx = W * H
+        self.accum = torch.zeros((self.npx, 4), dtype=torch.float32, device=device)
+        self.fd = torch.zeros(self.npx * 40, dtype=torch.uint8, device=device)
+        self.path_capacity = path_capacity
+        self.paths = torch.empty(path_capacity * 8, dtype=torch.uint8, device=device)
+        self.paths_tmp = torch.empty(path_capacity * 8, dtype=torch.uint8, device=device)
+        self.indexed = torch.empty(path_capacity, dtype=torch.int64, device=device)
+        self.indexed_tmp = torch.empty(path_capacity, dtype=torch.int64, device=device)
+        self.counter = torch.zeros(1, dtype=torch.int32, device=device)
+        self.status = torch.zeros(1, dtype=torch.int32, device=device)
+        self.stats = torch.zeros(3, dtype=torch.int64, device=device)
+
+
+def solve_primary(ds: DeviceScene, frame: Frame, iteration: int = 0, lens=(0.6, 0.05, 0.0), stream=None):
+    sc = ds.scene
+    g = ray_generator(sc)
+    l = _lib.LensParams(*[float(x) for x in lens])
+    _lib.call("pz_solve_primary", _vp(frame.accum), _vp(frame.fd), C.c_int(sc.width), C.c_int(sc.height), C.byref(g),
+              C.byref(l), _vp(ds.internals), _vp(ds.root_dev), _vp(ds.tris), _vp(ds.attribs), _lib.f3(sc.p_light),
+              C.c_float(sc.light_intensity), C.c_float(sc.radiance_clamp), C.c_float(sc.cauchy_a),
+              C.c_float(sc.cauchy_b), _lib.f3(sc.albedo), C.c_int(iteration), _vp(frame.status),
+              C.c_void_p(_stream(stream)))
+
+
+def lookup_flatten(frame: Frame, cache: PathCache, events: int, stream=None) -> int:
+    """lookupFlatten + the count read-back of the reference (pk.h:1486-1510).  Returns n_paths."""
+    frame.counter.zero_()
+    _lib.call("pz_lookup_flatten", C.c_uint32(events), _vp(frame.paths), _vp(frame.indexed), _vp(frame.counter),
+              C.c_uint32(frame.path_capacity), _vp(frame.fd), C.c_int(frame.npx), _vp(cache.buf),
+              C.c_uint32(cache.capacity), C.c_float(cache.step), C.c_void_p(_stream(stream)))
+    return min(int(frame.counter.item()) & 0xFFFFFFFF, frame.path_capacity)
+
+
+def sort_and_reorder(frame: Frame, n_paths: int, sorter: OnesweepSort, stream=None):
+    """Tuple-coherence sort (pk.h:1526) and reorderSpecularPath; the result is in frame.paths."""
+    if n_paths == 0:
+        return
+    sorter.sort(frame.indexed, None, frame.indexed_tmp, None, n_paths, 0, 32, stream)
+    _lib.call("pz_reorder_specular_paths", _vp(frame.indexed), _vp(frame.paths_tmp), _vp(frame.paths),
+              C.c_uint32(n_paths), C.c_void_p(_stream(stream)))
+    frame.paths, frame.paths_tmp = frame.paths_tmp, frame.paths
+
+
+def solve_desc(ds: DeviceScene, frame: Frame, cache: PathCache, events_str: str, n_paths: int, spectral=None,
+               etas=None, stats=None, max_iterations=32, cost_tolerance=1e-10, early_term_warmup=1):
+    from .scenes import event_descriptor
+    sc = ds.scene
+    d = _lib.SolveDesc()
+    d.K = len(events_str)
+    d.events = event_descriptor(events_str)
+    d.paths = frame.paths.data_ptr()
+    d.n_paths = n_paths
+    d.first_diffuse = frame.fd.data_ptr()
+    d.internals = ds.internals.data_ptr()
+    d.root = ds.root_dev.data_ptr()
+    d.triangles = ds.tris.data_ptr()
+    d.attribs = ds.attribs.data_ptr()
+    d.cache = cache.buf.data_ptr()
+    d.cache_capacity = cache.capacity
+    d.cell_step = cache.step
+    d.p_light = _lib.f3(sc.p_light)
+    d.light_intensity = sc.light_intensity
+    d.radiance_clamp = sc.radiance_clamp
+    d.cauchy_a = sc.cauchy_a
+    d.cauchy_b = sc.cauchy_b
+    d.accum = frame.accum.data_ptr()
+    d.spectral = spectral.data_ptr() if spectral is not None else None
+    d.etas = etas.data_ptr() if etas is not None else None
+    d.n_bins = sc.n_bins if spectral is not None else 1
+    d.max_iterations = max_iterations
+    d.cost_tolerance = cost_tolerance
+    d.early_term_warmup = early_term_warmup
+    d.stats = stats.data_ptr() if stats is not None else None
+    return d
+
+
+def solve_specular_plain(desc, stream=None):
+    _lib.call("pz_solve_specular_plain", C.byref(desc), C.c_void_p(_stream(stream)))
+
+
+def resolve_spectral(spectral, scene, rgb=None, pixels=None, stream=None):
+    _lib.call("pz_resolve_spectral", _vp(rgb), _vp(pixels), _vp(spectral), C.c_int(scene.width * scene.height),
+              C.c_int(scene.n_bins), C.c_float(scene.lambda_min), C.c_float(scene.lambda_max), _lib.f3(scene.albedo),
+              C.c_void_p(_stream(stream)))

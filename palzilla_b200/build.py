@@ -28,7 +28,12 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = {
     "pz_sort.cu": [],
     "pz_bvh.cu": ["-fmad=false"],
+    "pz_trace.cu": ["-fmad=false"],
+    "pz_photon.cu": ["-fmad=false"],
+    "pz_frame.cu": ["-fmad=false"],
+    "pz_solve.cu": [],
     "pz_capi.cu": [],
+    "pz_capi_frame.cu": [],
 }
 
 

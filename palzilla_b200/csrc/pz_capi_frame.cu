@@ -1,0 +1,234 @@
+// pz_capi_frame.cu -- C ABI for ray queries, PathCache, photons, eye pass, work list,
+// plain specular solve and resolve (include/palzilla_b200.h).
+#include <cmath>
+
+#include "pz_cache.cuh"
+#include "pz_capi_internal.h"
+#include "pz_frame.cuh"
+#include "pz_photon.cuh"
+#include "pz_solve.cuh"
+#include "pz_trace_api.cuh"
+
+using namespace pz;
+
+namespace {
+inline cudaStream_t S(pz_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+inline float3 F3(pz_float3 v) { return make_float3(v.x, v.y, v.z); }
+inline bool pow2(uint32_t x) { return x && !(x & (x - 1)); }
+inline int done(cudaError_t e, const char* where)
+{
+    if (e != cudaSuccess) return cuda_fail(e, where);
+    clear_error();
+    return PZ_OK;
+}
+}  // namespace
+
+extern "C" int pz_trace_closest(const pz_internal_node* internals_dev, const uint32_t* root_dev,
+                                const pz_triangle* triangles_dev, int n_rays, const float* ro_dev, const float* rd_dev,
+                                float* t_dev, float* uv_dev, uint32_t* tri_dev, float* ng_dev, uint32_t* status_dev,
+                                pz_stream_t stream)
+{
+    if (n_rays < 0 || (n_rays > 0 && (!root_dev || !triangles_dev || !ro_dev || !rd_dev || !t_dev)))
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_trace_closest: bad argument");
+    return done(launch_trace_closest(reinterpret_cast<const Node*>(internals_dev), root_dev,
+                                     reinterpret_cast<const Tri*>(triangles_dev), (uint32_t)n_rays, ro_dev, rd_dev,
+                                     t_dev, uv_dev, tri_dev, ng_dev, status_dev, S(stream)),
+                "pz_trace_closest");
+}
+
+extern "C" int pz_trace_any(const pz_internal_node* internals_dev, const uint32_t* root_dev,
+                            const pz_triangle* triangles_dev, int n_rays, const float* ro_dev, const float* rd_dev,
+                            const float* tmax_dev, uint8_t* hit_dev, pz_stream_t stream)
+{
+    if (n_rays < 0 || (n_rays > 0 && (!root_dev || !triangles_dev || !ro_dev || !rd_dev || !tmax_dev || !hit_dev)))
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_trace_any: bad argument");
+    return done(launch_trace_any(reinterpret_cast<const Node*>(internals_dev), root_dev,
+                                 reinterpret_cast<const Tri*>(triangles_dev), (uint32_t)n_rays, ro_dev, rd_dev,
+                                 tmax_dev, hit_dev, S(stream)),
+                "pz_trace_any");
+}
+
+// ---------------------------------------------------------------- PathCache
+extern "C" size_t pz_path_cache_bytes(uint32_t capacity) { return pow2(capacity) ? cache_bytes(capacity) : 0; }
+
+extern "C" int pz_path_cache_clear(void* cache_dev, uint32_t capacity, pz_stream_t stream)
+{
+    if (!cache_dev || !pow2(capacity)) return fail(PZ_ERR_INVALID_ARGUMENT, "pz_path_cache_clear: bad argument");
+    CacheView c = cache_view(cache_dev, capacity, 0.0f);
+    cudaError_t e = cudaMemsetAsync(c.h, 0, sizeof(CacheHeader), S(stream));
+    if (e == cudaSuccess) e = cudaMemsetAsync(c.hash, 0, sizeof(uint32_t) * (size_t)capacity, S(stream));
+    return done(e, "pz_path_cache_clear");
+}
+
+extern "C" int pz_path_cache_views(void* cache_dev, uint32_t capacity, uint32_t** hash_dev, uint32_t** cell_dev,
+                                   uint32_t** events_dev, int32_t** tris_dev, float** params_dev, uint32_t** count_dev)
+{
+    if (!cache_dev || !pow2(capacity)) return fail(PZ_ERR_INVALID_ARGUMENT, "pz_path_cache_views: bad argument");
+    CacheView c = cache_view(cache_dev, capacity, 0.0f);
+    if (hash_dev) *hash_dev = c.hash;
+    if (cell_dev) *cell_dev = c.cell;
+    if (events_dev) *events_dev = c.event;
+    if (tris_dev) *tris_dev = reinterpret_cast<int32_t*>(c.tris);
+    if (params_dev) *params_dev = reinterpret_cast<float*>(c.params);
+    if (count_dev) *count_dev = &c.h->count;
+    clear_error();
+    return PZ_OK;
+}
+
+// ---------------------------------------------------------------- photons
+extern "C" int pz_photon_trace(const pz_internal_node* internals_dev, const uint32_t* root_dev,
+                               const pz_triangle* triangles_dev, const pz_triangle_attrib* attribs_dev, int n_triangles,
+                               int photons_per_triangle, pz_float3 p_light, float eta_min, float eta_max, int iteration,
+                               float min_throughput, void* cache_dev, uint32_t cache_capacity, float cell_step,
+                               pz_photon_record* records_dev, pz_stream_t stream)
+{
+    if (n_triangles < 0 || photons_per_triangle < 0 || !root_dev || (n_triangles > 0 && (!triangles_dev || !attribs_dev)))
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_photon_trace: bad argument");
+    if (cache_dev && (!pow2(cache_capacity) || !(cell_step > 0.0f)))
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_photon_trace: cache capacity must be a power of two, step > 0");
+    CacheView c{};
+    if (cache_dev) c = cache_view(cache_dev, cache_capacity, cell_step);
+    return done(launch_photons(reinterpret_cast<const Node*>(internals_dev), root_dev,
+                               reinterpret_cast<const Tri*>(triangles_dev), reinterpret_cast<const Attrib*>(attribs_dev),
+                               (uint32_t)n_triangles, (uint32_t)photons_per_triangle, F3(p_light), eta_min, eta_max,
+                               iteration, min_throughput, c, reinterpret_cast<PhotonRecord*>(records_dev), S(stream)),
+                "pz_photon_trace");
+}
+
+// ---------------------------------------------------------------- eye pass
+extern "C" void pz_ray_generator_lookat(pz_ray_generator* g, pz_float3 eye, pz_float3 center, pz_float3 up, float fovy,
+                                        int width, int height)
+{
+    // camera.h:10-22 on the host; 1/sqrt with correctly rounded operations as the
+    // reference's host normalize, and the double-precision tan the reference calls.
+    auto nrm = [](pz_float3 v) {
+        float inv = 1.0f / std::sqrt(v.x * v.x + v.y * v.y + v.z * v.z);
+        return pz_float3{v.x * inv, v.y * inv, v.z * inv};
+    };
+    auto crs = [](pz_float3 a, pz_float3 b) {
+        return pz_float3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+    };
+    pz_float3 f = nrm(pz_float3{center.x - eye.x, center.y - eye.y, center.z - eye.z});
+    pz_float3 s = nrm(crs(f, up));
+    pz_float3 u = crs(s, f);
+    float ty = (float)std::tan((double)(fovy * 0.5f));
+    float tx = ty / (float)height * (float)width;
+    g->origin = eye;
+    g->right = pz_float3{s.x * tx, s.y * tx, s.z * tx};
+    g->up = pz_float3{u.x * ty, u.y * ty, u.z * ty};
+}
+
+extern "C" int pz_solve_primary(float* accum_dev, pz_first_diffuse* first_diffuse_dev, int width, int height,
+                                const pz_ray_generator* gen, const pz_lens_params* lens,
+                                const pz_internal_node* internals_dev, const uint32_t* root_dev,
+                                const pz_triangle* triangles_dev, const pz_triangle_attrib* attribs_dev,
+                                pz_float3 p_light, float light_intensity, float radiance_clamp, float cauchy_a,
+                                float cauchy_b, pz_float3 albedo, int iteration, uint32_t* status_dev,
+                                pz_stream_t stream)
+{
+    if (width < 0 || height < 0 || !gen || !accum_dev || !first_diffuse_dev || !root_dev || !triangles_dev ||
+        !attribs_dev)
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_solve_primary: bad argument");
+    RayGen g{F3(gen->origin), F3(gen->right), F3(gen->up)};
+    Lens l{0.6f, 0.05f, 0.0f};
+    if (lens) l = Lens{lens->distance, lens->thickness, lens->R};
+    return done(launch_primary(reinterpret_cast<float4*>(accum_dev), reinterpret_cast<FirstDiffuse*>(first_diffuse_dev),
+                               width, height, g, l, reinterpret_cast<const Node*>(internals_dev), root_dev,
+                               reinterpret_cast<const Tri*>(triangles_dev), reinterpret_cast<const Attrib*>(attribs_dev),
+                               F3(p_light), light_intensity, radiance_clamp, cauchy_a, cauchy_b, F3(albedo), iteration,
+                               status_dev, S(stream)),
+                "pz_solve_primary");
+}
+
+// ---------------------------------------------------------------- work list
+extern "C" int pz_lookup_flatten(uint32_t events, pz_specular_path* paths_dev, uint64_t* indexed_dev,
+                                 uint32_t* counter_dev, uint32_t capacity, const pz_first_diffuse* first_diffuse_dev,
+                                 int n_pixels, void* cache_dev, uint32_t cache_capacity, float cell_step,
+                                 pz_stream_t stream)
+{
+    if (n_pixels < 0 || !paths_dev || !indexed_dev || !counter_dev || !first_diffuse_dev || !cache_dev ||
+        !pow2(cache_capacity) || !(cell_step > 0.0f))
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_lookup_flatten: bad argument");
+    return done(launch_lookup(events, reinterpret_cast<SpecularPath*>(paths_dev),
+                              reinterpret_cast<unsigned long long*>(indexed_dev), counter_dev, capacity,
+                              reinterpret_cast<const FirstDiffuse*>(first_diffuse_dev), n_pixels,
+                              cache_view(cache_dev, cache_capacity, cell_step), S(stream)),
+                "pz_lookup_flatten");
+}
+
+extern "C" int pz_reorder_specular_paths(const uint64_t* indexed_dev, pz_specular_path* dst_dev,
+                                         const pz_specular_path* src_dev, uint32_t n, pz_stream_t stream)
+{
+    if (n > 0 && (!indexed_dev || !dst_dev || !src_dev))
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_reorder_specular_paths: bad argument");
+    return done(launch_reorder(reinterpret_cast<const unsigned long long*>(indexed_dev),
+                               reinterpret_cast<SpecularPath*>(dst_dev), reinterpret_cast<const SpecularPath*>(src_dev),
+                               n, S(stream)),
+                "pz_reorder_specular_paths");
+}
+
+// ---------------------------------------------------------------- solve
+namespace pz {
+int solve_args_from_desc(const pz_solve_desc* d, SolveArgs* a, const char* who)
+{
+    if (!d) return fail(PZ_ERR_INVALID_ARGUMENT, "%s: null descriptor", who);
+    if (d->K < 1 || d->K > 4) return fail(PZ_ERR_INVALID_ARGUMENT, "%s: K must be 1..4 (got %d)", who, d->K);
+    if ((int)(d->events >> 24) != d->K)
+        return fail(PZ_ERR_INVALID_ARGUMENT, "%s: event descriptor size %u != K %d", who, d->events >> 24, d->K);
+    if (!d->cache || !pow2(d->cache_capacity) || !(d->cell_step > 0.0f))
+        return fail(PZ_ERR_INVALID_ARGUMENT, "%s: bad cache", who);
+    if (d->n_paths && (!d->paths || !d->first_diffuse || !d->root || !d->triangles || !d->attribs))
+        return fail(PZ_ERR_INVALID_ARGUMENT, "%s: null buffer", who);
+    if (d->spectral && (d->n_bins < 1 || !d->etas)) return fail(PZ_ERR_INVALID_ARGUMENT, "%s: bins need etas", who);
+    if (!d->spectral && !d->accum) return fail(PZ_ERR_INVALID_ARGUMENT, "%s: need accum or spectral", who);
+    a->accum = reinterpret_cast<float4*>(d->accum);
+    a->spectral = d->spectral;
+    a->etas = d->etas;
+    a->nBins = d->spectral ? d->n_bins : 1;
+    a->paths = reinterpret_cast<const SpecularPath*>(d->paths);
+    a->nPaths = d->n_paths;
+    a->fds = reinterpret_cast<const FirstDiffuse*>(d->first_diffuse);
+    a->nodes = reinterpret_cast<const Node*>(d->internals);
+    a->root = d->root;
+    a->tris = reinterpret_cast<const Tri*>(d->triangles);
+    a->attribs = reinterpret_cast<const Attrib*>(d->attribs);
+    a->p_light = F3(d->p_light);
+    a->lightIntensity = d->light_intensity;
+    a->radianceClamp = d->radiance_clamp;
+    a->cache = cache_view(d->cache, d->cache_capacity, d->cell_step);
+    a->events = d->events;
+    a->cauchyA = d->cauchy_a;
+    a->cauchyB = d->cauchy_b;
+    a->maxIterations = d->max_iterations > 0 ? d->max_iterations : 32;
+    a->costTolerance = d->cost_tolerance > 0.0f ? d->cost_tolerance : 1.0e-10f;
+    a->earlyTermWarmUp = d->early_term_warmup;
+    a->stats = d->stats;
+    return PZ_OK;
+}
+}  // namespace pz
+
+extern "C" int pz_solve_specular_plain(const pz_solve_desc* desc, pz_stream_t stream)
+{
+    SolveArgs a;
+    int r = solve_args_from_desc(desc, &a, "pz_solve_specular_plain");
+    if (r != PZ_OK) return r;
+    return done(launch_solve_plain(desc->K, desc->spectral != nullptr, a, S(stream)), "pz_solve_specular_plain");
+}
+
+// ---------------------------------------------------------------- resolve
+extern "C" int pz_resolve(uint32_t* pixels_dev, const float* accum_dev, int n_pixels, pz_stream_t stream)
+{
+    if (n_pixels < 0 || (n_pixels > 0 && (!pixels_dev || !accum_dev)))
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_resolve: bad argument");
+    return done(launch_pack(pixels_dev, reinterpret_cast<const float4*>(accum_dev), n_pixels, S(stream)), "pz_resolve");
+}
+
+extern "C" int pz_resolve_spectral(float* rgb_dev, uint32_t* pixels_dev, const float* spectral_dev, int n_pixels,
+                                   int n_bins, float lambda_min, float lambda_max, pz_float3 albedo, pz_stream_t stream)
+{
+    if (n_pixels < 0 || n_bins < 1 || (n_pixels > 0 && !spectral_dev))
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_resolve_spectral: bad argument");
+    return done(launch_resolve_spectral(reinterpret_cast<float4*>(rgb_dev), pixels_dev, spectral_dev, n_pixels, n_bins,
+                                        lambda_min, lambda_max, F3(albedo), S(stream)),
+                "pz_resolve_spectral");
+}

@@ -121,6 +121,7 @@ PZ_D float any_hit(const Node* __restrict__ nodes, const Tri* __restrict__ tris,
                 best = t;
                 break;
             }
+            if (prev == kInvalidNode) break;  // the root is a leaf (one-triangle scene)
             const NodeView p = load_node(nodes, node_idx(prev));
             if (p.c0 == curr) {  // just go to the sibling side of prev
                 const uint32_t tmp = curr;
