@@ -206,6 +206,7 @@ typedef struct pz_solve_desc {
     float cost_tolerance;                  /* 1e-10 */
     int early_term_warmup;                 /* 1 */
     unsigned long long* stats;             /* device u64[3]: items solved, converged, contributing (or NULL) */
+    int exact_arithmetic;                  /* 1: no FMA contraction (bit-compatible with the CPU oracle) */
 } pz_solve_desc;
 /* One thread per work item, one launch per call: the reference's plain structure. */
 PZ_API int pz_solve_specular_plain(const pz_solve_desc* desc, pz_stream_t stream);

@@ -40,7 +40,7 @@ class SolveDesc(C.Structure):
                 ("cache_capacity", u32), ("cell_step", f32), ("p_light", Float3), ("light_intensity", f32),
                 ("radiance_clamp", f32), ("cauchy_a", f32), ("cauchy_b", f32), ("accum", vp), ("spectral", vp),
                 ("etas", vp), ("n_bins", i32), ("max_iterations", i32), ("cost_tolerance", f32),
-                ("early_term_warmup", i32), ("stats", vp)]
+                ("early_term_warmup", i32), ("stats", vp), ("exact_arithmetic", i32)]
 
 
 def f3(v) -> Float3:

@@ -261,7 +261,7 @@ def sort_and_reorder(frame: Frame, n_paths: int, sorter: OnesweepSort, stream=No
 
 
 def solve_desc(ds: DeviceScene, frame: Frame, cache: PathCache, events_str: str, n_paths: int, spectral=None,
-               etas=None, stats=None, max_iterations=32, cost_tolerance=1e-10, early_term_warmup=1):
+               etas=None, stats=None, max_iterations=32, cost_tolerance=1e-10, early_term_warmup=1, exact=False):
     from .scenes import event_descriptor
     sc = ds.scene
     d = _lib.SolveDesc()
@@ -290,6 +290,7 @@ def solve_desc(ds: DeviceScene, frame: Frame, cache: PathCache, events_str: str,
     d.cost_tolerance = cost_tolerance
     d.early_term_warmup = early_term_warmup
     d.stats = stats.data_ptr() if stats is not None else None
+    d.exact_arithmetic = 1 if exact else 0
     return d
 
 

@@ -24,16 +24,17 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
           "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]
 
-# translation unit -> extra flags
+# object name -> (source, extra flags)
 UNITS = {
-    "pz_sort.cu": [],
-    "pz_bvh.cu": ["-fmad=false"],
-    "pz_trace.cu": ["-fmad=false"],
-    "pz_photon.cu": ["-fmad=false"],
-    "pz_frame.cu": ["-fmad=false"],
-    "pz_solve.cu": [],
-    "pz_capi.cu": [],
-    "pz_capi_frame.cu": [],
+    "pz_sort": ("pz_sort.cu", []),
+    "pz_bvh": ("pz_bvh.cu", ["-fmad=false"]),
+    "pz_trace": ("pz_trace.cu", ["-fmad=false"]),
+    "pz_photon": ("pz_photon.cu", ["-fmad=false"]),
+    "pz_frame": ("pz_frame.cu", ["-fmad=false"]),
+    "pz_solve": ("pz_solve.cu", []),
+    "pz_solve_exact": ("pz_solve.cu", ["-fmad=false", "-DPZ_SOLVE_EXACT"]),
+    "pz_capi": ("pz_capi.cu", []),
+    "pz_capi_frame": ("pz_capi_frame.cu", []),
 }
 
 
@@ -49,9 +50,9 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
     headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + \
         glob.glob(os.path.join(ROOT, "include", "*.h"))
     objs, procs = [], []
-    for unit, flags in UNITS.items():
-        src = os.path.join(CSRC, unit)
-        obj = os.path.join(OBJ, unit.replace(".cu", ".o"))
+    for unit, (srcname, flags) in UNITS.items():
+        src = os.path.join(CSRC, srcname)
+        obj = os.path.join(OBJ, unit + ".o")
         objs.append(obj)
         if _newer(obj, [src] + headers + [__file__]):
             cmd = [NVCC] + ARCH + COMMON + flags + ["-c", src, "-o", obj]

@@ -212,7 +212,8 @@ extern "C" int pz_solve_specular_plain(const pz_solve_desc* desc, pz_stream_t st
     SolveArgs a;
     int r = solve_args_from_desc(desc, &a, "pz_solve_specular_plain");
     if (r != PZ_OK) return r;
-    return done(launch_solve_plain(desc->K, desc->spectral != nullptr, a, S(stream)), "pz_solve_specular_plain");
+    auto launch = desc->exact_arithmetic ? launch_solve_plain_exact : launch_solve_plain;
+    return done(launch(desc->K, desc->spectral != nullptr, a, S(stream)), "pz_solve_specular_plain");
 }
 
 // ---------------------------------------------------------------- resolve

@@ -6,11 +6,24 @@
 // barycentrics: Newton solve, admissibility + visibility, dAdw, clamped contribution
 // accumulated with atomics (RGB in reference mode, one spectral bin in binned mode).
 // This is the structure the batched persistent solver is measured against.
+//
+// The unit is compiled twice: as is (FMA contraction on: the performance baseline) and
+// with -DPZ_SOLVE_EXACT -fmad=false, which gives results bit-compatible with the CPU
+// oracle for the parity tests.
 #include "pz_frame.cuh"
 #include "pz_solve.cuh"
 #include "pz_solver.cuh"
 
+#ifdef PZ_SOLVE_EXACT
+#define PZ_SOLVE_NS exact
+#define PZ_SOLVE_LAUNCH launch_solve_plain_exact
+#else
+#define PZ_SOLVE_NS fast
+#define PZ_SOLVE_LAUNCH launch_solve_plain
+#endif
+
 namespace pz {
+namespace PZ_SOLVE_NS {
 
 using solver::V3;
 
@@ -84,8 +97,11 @@ static cudaError_t launch_k(const SolveArgs& a, cudaStream_t s)
     return cudaGetLastError();
 }
 
-cudaError_t launch_solve_plain(int K, bool binned, const SolveArgs& a, cudaStream_t s)
+}  // namespace PZ_SOLVE_NS
+
+cudaError_t PZ_SOLVE_LAUNCH(int K, bool binned, const SolveArgs& a, cudaStream_t s)
 {
+    using namespace PZ_SOLVE_NS;
     switch (K * 2 + (binned ? 1 : 0)) {
         case 2: return launch_k<1, false>(a, s);
         case 3: return launch_k<1, true>(a, s);
@@ -99,6 +115,7 @@ cudaError_t launch_solve_plain(int K, bool binned, const SolveArgs& a, cudaStrea
     return cudaErrorInvalidValue;
 }
 
+#ifndef PZ_SOLVE_EXACT
 // ---------------------------------------------------------------- resolve
 PZ_D float srgb_oetf(float r)  // pk.h:1023-1031
 {
@@ -155,5 +172,7 @@ cudaError_t launch_resolve_spectral(float4* rgb, uint32_t* pixels, const float* 
     k_resolve_spectral<<<(n + 255) / 256, 256, 0, s>>>(rgb, pixels, spectral, n, nBins, lambdaMin, lambdaMax, albedo);
     return cudaGetLastError();
 }
+
+#endif  // PZ_SOLVE_EXACT
 
 }  // namespace pz

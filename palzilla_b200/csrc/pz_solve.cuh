@@ -29,6 +29,8 @@ struct SolveArgs {
 };
 
 cudaError_t launch_solve_plain(int K, bool binned, const SolveArgs& a, cudaStream_t s);
+// the same kernels without FMA contraction (bit-compatible with the CPU oracle)
+cudaError_t launch_solve_plain_exact(int K, bool binned, const SolveArgs& a, cudaStream_t s);
 cudaError_t launch_pack(uint32_t* pixels, const float4* accum, int n, cudaStream_t s);
 cudaError_t launch_resolve_spectral(float4* rgb, uint32_t* pixels, const float* spectral, int n, int nBins,
                                     float lambdaMin, float lambdaMax, float3 albedo, cudaStream_t s);

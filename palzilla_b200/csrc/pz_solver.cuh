@@ -49,10 +49,9 @@ template <class T> PZ_HD D<T> operator+(D<T> a, D<T> b) { return {a.v + b.v, a.g
 template <class T> PZ_HD D<T> operator-(D<T> a, D<T> b) { return {a.v - b.v, a.g - b.g}; }
 template <class T> PZ_HD D<T> operator-(D<T> a) { return {-a.v, -a.g}; }
 template <class T> PZ_HD D<T> operator*(D<T> a, D<T> b) { return {a.v * b.v, a.g * b.v + b.g * a.v}; }
-template <class T> PZ_HD D<T> operator/(D<T> a, D<T> b)
+template <class T> PZ_HD D<T> operator/(D<T> a, D<T> b)  // saka.h:77-83
 {
-    const T inv = T(1) / b.v;
-    return {a.v * inv, (a.g - a.v * inv * b.g) * inv};
+    return {a.v / b.v, a.g * (T(1) / b.v) + b.g * (-a.v / (b.v * b.v))};
 }
 template <class T> PZ_D D<T> dsqrt(D<T> a)
 {

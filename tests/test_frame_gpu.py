@@ -140,40 +140,50 @@ def test_eye_pass_and_lookup(orc, lens, lens_bvh):
     assert got == sorted(map(tuple, pairs_o.tolist()))
 
 
-def _render_plain(ds, sc, frame, cache, spectral, stats):
+def _render_plain(ds, sc, frame, cache, spectral, stats, exact=True):
     ev = S.event_descriptor(sc.events)
     n = A.lookup_flatten(frame, cache, ev)
     A.sort_and_reorder(frame, n, A.OnesweepSort())
     etas = torch.from_numpy(sc.bin_etas()).cuda()
-    d = A.solve_desc(ds, frame, cache, sc.events, n, spectral=spectral, etas=etas, stats=stats)
+    d = A.solve_desc(ds, frame, cache, sc.events, n, spectral=spectral, etas=etas, stats=stats, exact=exact)
     A.solve_specular_plain(d)
     return n
 
 
+def _rel(a, b):
+    return float(np.sqrt(((a - b) ** 2).mean()) / max(np.sqrt((b ** 2).mean()), 1e-30))
+
+
 @pytest.mark.parametrize("events", ["T", "TT"])
 def test_plain_solve_spectral_image(orc, events):
+    """Exact-arithmetic variant: equal to the float oracle up to atomic-add order (1e-5);
+    FMA variant: within 2e-3 (marginal paths at triangle edges can flip accept/reject);
+    both against FP64 within 1e-2 (the FP32 solve's own error, reported)."""
     sc = S.lens_scene(side=40, seed=21, width=96, height=96, n_bins=8, events=events)
     ds = A.DeviceScene(sc)
     frame = A.Frame(sc, path_capacity=1 << 22)
     A.solve_primary(ds, frame, iteration=0)
     cache = A.PathCache(capacity=1 << 20, step=sc.cell_step)
     A.photon_trace(ds, cache, iteration=0)
-    spectral = torch.zeros((sc.width * sc.height, sc.n_bins), device="cuda")
-    stats = torch.zeros(3, dtype=torch.int64, device="cuda")
-    n = _render_plain(ds, sc, frame, cache, spectral, stats)
-    torch.cuda.synchronize()
+    imgs, stats = {}, {}
+    for exact in (True, False):
+        spectral = torch.zeros((sc.width * sc.height, sc.n_bins), device="cuda")
+        st = torch.zeros(3, dtype=torch.int64, device="cuda")
+        n = _render_plain(ds, sc, frame, cache, spectral, st, exact=exact)
+        torch.cuda.synchronize()
+        imgs[exact], stats[exact] = spectral.cpu().numpy(), st.cpu().numpy()
     assert n > 0
-    st = stats.cpu().numpy()
-    assert st[0] == n * sc.n_bins and st[2] > 0
-    # oracle over the same work list (the GPU's sorted pairs and cache)
+    assert stats[True][0] == n * sc.n_bins and stats[True][2] > 0
     gc = cache.to_host()
     pairs = frame.paths[: n * 8].cpu().numpy().view(np.int32).reshape(-1, 2).copy()
     fd = frame.fd.cpu().numpy().view(np.float32).reshape(-1, 10)
     bvh = orc.build_bvh(sc.tris)
     img_f, st_f = orc.render_pairs(len(events), pairs, gc, fd, bvh, sc, sc.bin_etas())
     img_d, _ = orc.render_pairs(len(events), pairs, gc, fd, bvh, sc, sc.bin_etas(), dtype=np.float64)
-    g = spectral.cpu().numpy()
-    rel = lambda a, b: float(np.sqrt(((a - b) ** 2).mean()) / max(np.sqrt((b ** 2).mean()), 1e-30))
-    assert rel(g, img_f) <= 1e-3, rel(g, img_f)
-    assert rel(g, img_d) <= 1e-2, rel(g, img_d)   # FP32 vs FP64, reported in DESIGN
-    assert abs(int(st[2]) - int(st_f[2])) <= max(3, 0.002 * st_f[2])
+    assert np.array_equal(stats[True], st_f), (stats[True], st_f)
+    assert _rel(imgs[True], img_f) <= 1e-5, _rel(imgs[True], img_f)
+    assert _rel(imgs[False], img_f) <= 2e-3, _rel(imgs[False], img_f)
+    for exact in (True, False):
+        assert _rel(imgs[exact], img_d) <= 1e-2, _rel(imgs[exact], img_d)
+    print(f"\n[{events}] rel RMSE exact-vs-oracle {_rel(imgs[True], img_f):.2e}  fma-vs-oracle "
+          f"{_rel(imgs[False], img_f):.2e}  fp32-vs-fp64 {_rel(imgs[True], img_d):.2e}")
