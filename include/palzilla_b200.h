@@ -206,10 +206,32 @@ typedef struct pz_solve_desc {
     float cost_tolerance;                  /* 1e-10 */
     int early_term_warmup;                 /* 1 */
     unsigned long long* stats;             /* device u64[3]: items solved, converged, contributing (or NULL) */
-    int exact_arithmetic;                  /* 1: no FMA contraction (bit-compatible with the CPU oracle) */
+    int exact_arithmetic;                  /* plain solve: 1 = no FMA contraction (bit-compatible with the CPU oracle) */
+    float polish_det;                      /* batched solve: FP64 polish of roots whose relative determinant
+                                              prod|R_ii| / max|R_ii|^(2K) is below this; 0 = 1e-6, < 0 = never */
+    int continuation;                      /* batched solve: 1 = refine each bin from its predicted root
+                                              (faster; roots near triangle edges are accepted more often
+                                              than the reference's Newton path accepts them) */
 } pz_solve_desc;
 /* One thread per work item, one launch per call: the reference's plain structure. */
 PZ_API int pz_solve_specular_plain(const pz_solve_desc* desc, pz_stream_t stream);
+
+/* Batched persistent solve (binned mode only, n_bins <= 64): the same work items and
+ * per-bin semantics as pz_solve_specular_plain, scheduled for the GPU -- persistent
+ * warps, the root of every bin predicted from one centre-bin solve and its derivative
+ * in eta, bins outside the triangles rejected without a solve, warp-shared visibility
+ * queries, FP64 polish of ill-conditioned roots.  n_paths_dev (device u32, e.g. the
+ * lookup counter) gives the item count on the device so no host round trip is needed
+ * (desc->n_paths is then the capacity); NULL uses desc->n_paths.  blocks_per_sm <= 0
+ * picks the default.  scratch: pz_solve_batched_scratch_bytes(K, capacity) bytes. */
+PZ_API size_t pz_solve_batched_scratch_bytes(int K, uint64_t max_paths);
+/* After a batched solve: the scratch header holds u64 diagnostics at byte offset 64:
+ * items skipped by prediction, predicted, plain fallback, per-bin Newton solves, FP64
+ * polishes, visibility-query overflows, visibility candidates, visibility queries,
+ * fallbacks because the centre solve did not converge, fallbacks because the predicted
+ * shift over the band was too large. */
+PZ_API int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32_t* n_paths_dev, void* scratch_dev,
+                                     size_t scratch_bytes, int blocks_per_sm, pz_stream_t stream);
 
 /* ---------------------------------------------------------------- resolve
  * pack (main_gpu.cu:499-513): accumulator / count -> sRGB OETF -> RGBA8. */

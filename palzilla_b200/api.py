@@ -261,7 +261,8 @@ def sort_and_reorder(frame: Frame, n_paths: int, sorter: OnesweepSort, stream=No
 
 
 def solve_desc(ds: DeviceScene, frame: Frame, cache: PathCache, events_str: str, n_paths: int, spectral=None,
-               etas=None, stats=None, max_iterations=32, cost_tolerance=1e-10, early_term_warmup=1, exact=False):
+               etas=None, stats=None, max_iterations=32, cost_tolerance=1e-10, early_term_warmup=1, exact=False,
+               polish_det=0.0, continuation=False):
     from .scenes import event_descriptor
     sc = ds.scene
     d = _lib.SolveDesc()
@@ -291,11 +292,31 @@ def solve_desc(ds: DeviceScene, frame: Frame, cache: PathCache, events_str: str,
     d.early_term_warmup = early_term_warmup
     d.stats = stats.data_ptr() if stats is not None else None
     d.exact_arithmetic = 1 if exact else 0
+    d.polish_det = polish_det
+    d.continuation = 1 if continuation else 0
     return d
 
 
 def solve_specular_plain(desc, stream=None):
     _lib.call("pz_solve_specular_plain", C.byref(desc), C.c_void_p(_stream(stream)))
+
+
+def solve_specular_batched(desc, scratch: Scratch, n_paths_dev=None, blocks_per_sm: int = 0, stream=None):
+    """Batched persistent solve; n_paths_dev (device int32 tensor) supplies the item count
+    on the device (desc.n_paths is then the capacity)."""
+    nbytes = _lib.lib().pz_solve_batched_scratch_bytes(desc.K, desc.n_paths)
+    buf = scratch.get(nbytes)
+    _lib.call("pz_solve_specular_batched", C.byref(desc), _vp(n_paths_dev), _vp(buf), C.c_size_t(buf.numel()),
+              C.c_int(blocks_per_sm), C.c_void_p(_stream(stream)))
+
+
+BATCH_COUNTERS = ("skipped", "predicted", "fallback", "newton_bins", "fp64_polish", "vis_overflow", "vis_candidates",
+                  "vis_queries", "fallback_noconv", "fallback_shift")
+
+
+def batched_counters(scratch: Scratch) -> dict:
+    v = scratch.buf[64:144].view(torch.int64).cpu().tolist()
+    return dict(zip(BATCH_COUNTERS, v))
 
 
 def resolve_spectral(spectral, scene, rgb=None, pixels=None, stream=None):

@@ -2,6 +2,7 @@
 // plain specular solve and resolve (include/palzilla_b200.h).
 #include <cmath>
 
+#include "pz_batched_api.cuh"
 #include "pz_cache.cuh"
 #include "pz_capi_internal.h"
 #include "pz_frame.cuh"
@@ -214,6 +215,42 @@ extern "C" int pz_solve_specular_plain(const pz_solve_desc* desc, pz_stream_t st
     if (r != PZ_OK) return r;
     auto launch = desc->exact_arithmetic ? launch_solve_plain_exact : launch_solve_plain;
     return done(launch(desc->K, desc->spectral != nullptr, a, S(stream)), "pz_solve_specular_plain");
+}
+
+extern "C" size_t pz_solve_batched_scratch_bytes(int K, uint64_t max_paths)
+{
+    if (K < 1 || K > 4) return 0;
+    return 256 + (size_t)max_paths * batched::record_bytes(K);
+}
+
+extern "C" int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32_t* n_paths_dev, void* scratch_dev,
+                                         size_t scratch_bytes, int blocks_per_sm, pz_stream_t stream)
+{
+    batched::BatchArgs b;
+    int r = solve_args_from_desc(desc, &b.s, "pz_solve_specular_batched");
+    if (r != PZ_OK) return r;
+    if (!desc->spectral || desc->n_bins < 1 || desc->n_bins > 64)
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_solve_specular_batched: binned mode with 1..64 bins required");
+    const size_t need = pz_solve_batched_scratch_bytes(desc->K, desc->n_paths);
+    if (!scratch_dev || scratch_bytes < need)
+        return fail(PZ_ERR_SCRATCH_TOO_SMALL, "pz_solve_specular_batched: scratch %zu < required %zu", scratch_bytes,
+                    need);
+    if (reinterpret_cast<uintptr_t>(scratch_dev) & 255)
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_solve_specular_batched: scratch needs 256-byte alignment");
+    char* base = static_cast<char*>(scratch_dev);
+    b.status = reinterpret_cast<uint32_t*>(base);
+    b.workCounter = reinterpret_cast<unsigned long long*>(base + 8);
+    b.recordCount = reinterpret_cast<unsigned long long*>(base + 16);
+    b.records = base + 256;
+    b.recordCapacity = desc->n_paths;
+    b.nPathsDev = n_paths_dev;
+    b.counters = reinterpret_cast<unsigned long long*>(base + 64);
+    b.polishDet = desc->polish_det < 0.0f ? 0.0 : (desc->polish_det == 0.0f ? 1.0e-6 : (double)desc->polish_det);
+    b.continuation = desc->continuation;
+    if (desc->n_paths == 0) { clear_error(); return PZ_OK; }
+    cudaError_t e = cudaMemsetAsync(base, 0, 256, S(stream));
+    if (e == cudaSuccess) e = batched::launch_solve_batched(desc->K, b, blocks_per_sm > 0 ? blocks_per_sm : 2, S(stream));
+    return done(e, "pz_solve_specular_batched");
 }
 
 // ---------------------------------------------------------------- resolve
