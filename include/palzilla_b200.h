@@ -212,6 +212,9 @@ typedef struct pz_solve_desc {
     int continuation;                      /* batched solve: 1 = refine each bin from its predicted root
                                               (faster; roots near triangle edges are accepted more often
                                               than the reference's Newton path accepts them) */
+    float fold_det;                        /* batched solve: items whose roots have a relative determinant
+                                              below this (near a fold of the caustic) are solved bin by bin
+                                              from the photon barycentrics; 0 = 1e-2, < 0 = never */
 } pz_solve_desc;
 /* One thread per work item, one launch per call: the reference's plain structure. */
 PZ_API int pz_solve_specular_plain(const pz_solve_desc* desc, pz_stream_t stream);

@@ -262,7 +262,7 @@ def sort_and_reorder(frame: Frame, n_paths: int, sorter: OnesweepSort, stream=No
 
 def solve_desc(ds: DeviceScene, frame: Frame, cache: PathCache, events_str: str, n_paths: int, spectral=None,
                etas=None, stats=None, max_iterations=32, cost_tolerance=1e-10, early_term_warmup=1, exact=False,
-               polish_det=0.0, continuation=False):
+               polish_det=0.0, continuation=False, fold_det=0.0):
     from .scenes import event_descriptor
     sc = ds.scene
     d = _lib.SolveDesc()
@@ -294,6 +294,7 @@ def solve_desc(ds: DeviceScene, frame: Frame, cache: PathCache, events_str: str,
     d.exact_arithmetic = 1 if exact else 0
     d.polish_det = polish_det
     d.continuation = 1 if continuation else 0
+    d.fold_det = fold_det
     return d
 
 

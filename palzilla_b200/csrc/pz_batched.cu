@@ -30,11 +30,19 @@
 namespace pz {
 namespace batched {
 
+// Compile-time choices measured by the variant sweep: lanes take the bins to solve in
+// rank order (1) or bin = lane + 32 * round (0); dAdw in one two-tangent pass (1) or two
+// single-tangent passes (0).
+#ifndef PZ_BATCHED_RANK
+#define PZ_BATCHED_RANK 0
+#endif
+#ifndef PZ_BATCHED_DADW2
+#define PZ_BATCHED_DADW2 1
+#endif
+
 constexpr int kWarpsPerBlock = 8;
 constexpr int kMaxCand = 32;
-constexpr float kMargin = 0.3f;      // barycentric margin for skipping a bin (> edge_eps 0.25)
 constexpr float kMaxShift = 0.5f;    // a larger predicted shift over the band falls back
-constexpr float kIllDet = 1.0e-2f;   // relative det below which an item is near a fold: per-bin solves
 constexpr float kDeep = 0.3f;        // a predicted root this far inside every triangle is refined, not re-solved
 
 // Phase-1 result of one work item that has bins to refine (global, compacted).
@@ -107,6 +115,30 @@ PZ_D T pre_throughput(const T* x, V3<T> p_beg, V3<T> p_end, const Chain<K>& ch, 
         nrm[i] = mk3((float)sn[i].x, (float)sn[i].y, (float)sn[i].z);
     }
     return thr;
+}
+
+// Chain vertex i (0 = light, K + 1 = receiver point) and its normal as
+// contributableThroughput builds them (pk.h:763-789), from the barycentrics.
+template <int K>
+PZ_D void chain_vertex(const Chain<K>& ch, const float* x, float3 p_light, float3 p_end, int i, float3& v, float3& n)
+{
+    auto vert = [&](int j) -> float3 {
+        if (j == 0) return p_light;
+        if (j == K + 1) return p_end;
+        const V3<float> q = vertex<float, K>(ch, x, j - 1);
+        return mk3(q.x, q.y, q.z);
+    };
+    v = vert(i);
+    if (i == 0) {
+        n = normalize(vert(1) - vert(0));
+    } else if (i == K + 1) {
+        n = normalize(vert(K) - vert(K + 1));
+    } else {
+        const float u = x[2 * (i - 1)], w = x[2 * (i - 1) + 1];
+        const V3<float> sn = vnormalize(v3f<float>(ch.n0[i - 1]) + v3f<float>(ch.ne0[i - 1]) * u +
+                                        v3f<float>(ch.ne1[i - 1]) * w);
+        n = mk3(sn.x, sn.y, sn.z);
+    }
 }
 
 // The shadow-ray segment of occluded() (pk.h:88-115): start and end points.
@@ -190,7 +222,11 @@ __device__ __noinline__ float dadw_out_of_line(const Chain<K>& ch, const float* 
 {
     const V3<float> L = v3f<float>(p_light);
     const V3<float> v0 = vertex<float, K>(ch, xs, 0);
+#if PZ_BATCHED_DADW2
+    return dadw2<float, K>(L, v0 - L, v3f<float>(p), ch, events, eta);
+#else
     return dadw<float, K>(L, v0 - L, v3f<float>(p), ch, events, eta);
+#endif
 }
 
 // ---------------------------------------------------------------- phase 1
@@ -266,7 +302,7 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
             }
             const float minDet = fminf(det, fminf(da, db));
             conv2 = ca && cb;
-            if (minDet < kIllDet) {
+            if (minDet < a.illDet) {
                 // near a fold of the root curve: plain per-bin solves, FP64 polish when near-singular
                 r.polish = (double)minDet < a.polishDet ? 1 : 0;
             } else if (ca && cb && finite && nonlin < kMaxShift) {
@@ -348,12 +384,21 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
 #pragma unroll
             for (int i = 0; i < 2 * K; i++) x0[i] = pp[i];
         }
+        // lanes take the bins to solve in rank order (the set bits of the item's mask)
+        const unsigned long long todo = r.mode == 2 ? (B == 64 ? ~0ull : ((1ull << B) - 1ull)) : r.mask;
+#if PZ_BATCHED_RANK
+        const int nTodo = __popcll(todo);
+        for (int round = 0; round * 32 < nTodo; round++) {
+            const int rank = lane + 32 * round;
+            const int b = rank < nTodo ? nth_bit64(todo, rank) : B;
+#else
         for (int round = 0; round * 32 < B; round++) {
-            const int b = lane + 32 * round;
+            const int b0 = lane + 32 * round;
+            const int b = (b0 < B && ((todo >> b0) & 1ull)) ? b0 : B;
+#endif
             float xs[2 * K];
             float thr = 0.0f;
-            float3 vtx[K + 2], nrm[K + 2];
-            if (b < B && (r.mode == 2 || ((r.mask >> b) & 1ull))) {
+            if (b < B) {
                 const float eta = a.s.etas[b];
                 const bool warm = r.mode == 1 && (a.continuation || ((r.warm >> b) & 1ull));
                 if (warm) {
@@ -372,6 +417,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
                     nConv++;
                     const bool polish = r.polish || (double)det < a.polishDet;
                     if (polish && a.counters) atomicAdd(a.counters + kCntPolish, 1ull);
+                    float3 vtx[K + 2], nrm[K + 2];
                     if (polish)
                         thr = polish_fp64<K>(xs, ch, a.s.p_light, fd.p, a.s.events, eta, vtx, nrm);
                     else
@@ -384,7 +430,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
                 if (!valid) break;
                 const int leader = __ffs(valid) - 1;
                 float3 sa = mk3(0.f, 0.f, 0.f), sb = mk3(0.f, 0.f, 0.f);
-                if (thr > 0.0f) shadow_segment(vtx[s], nrm[s], vtx[s + 1], nrm[s + 1], sa, sb);
+                if (thr > 0.0f) {
+                    float3 v0, n0, v1, n1;
+                    chain_vertex<K>(ch, xs, a.s.p_light, fd.p, s, v0, n0);
+                    chain_vertex<K>(ch, xs, a.s.p_light, fd.p, s + 1, v1, n1);
+                    shadow_segment(v0, n0, v1, n1, sa, sb);
+                }
                 const float3 ra = mk3(__shfl_sync(0xFFFFFFFFu, sa.x, leader), __shfl_sync(0xFFFFFFFFu, sa.y, leader),
                                       __shfl_sync(0xFFFFFFFFu, sa.z, leader));
                 const float3 rb = mk3(__shfl_sync(0xFFFFFFFFu, sb.x, leader), __shfl_sync(0xFFFFFFFFu, sb.y, leader),

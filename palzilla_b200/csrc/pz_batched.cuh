@@ -259,5 +259,83 @@ PZ_D bool newton(T* x, V3<T> p_beg, V3<T> p_end, const Chain<K>& ch, T eta, uint
     return false;
 }
 
+
+// dAdw (pk.h:844-930) with both ray-differential tangents carried in one pass; each
+// tangent follows the single-tangent operation sequence of the reference.
+template <class T, int K>
+PZ_D T dadw2(V3<T> ro, V3<T> rd, V3<T> p_end, const Chain<K>& ch, uint32_t events, T eta)
+{
+    rd = vnormalize(rd);
+    const T sign = copysign(T(1), rd.z);
+    const T a = T(-1) / (sign + rd.z);
+    const T bb = rd.x * rd.y * a;
+    const V3<T> T0 = v3<T>(T(1) + sign * rd.x * rd.x * a, sign * bb, -sign * rd.x);
+    const V3<T> T1 = v3<T>(bb, sign + rd.y * rd.y * a, -rd.y);
+    MD<T, 2> d0 = mconst<T, 2>(T(0)), d1 = mconst<T, 2>(T(0));
+    d0.g[0] = T(1);
+    d1.g[1] = T(1);
+    MD3<T, 2> ro_j = m3<T, 2>(ro);
+    MD3<T, 2> rd_j = m3<T, 2>(rd) + m3<T, 2>(T0) * d0 + m3<T, 2>(T1) * d1;
+#pragma unroll
+    for (int j = 0; j < K; j++) {
+        const V3<T> ng = v3f<T>(ch.ng[j]);
+        const V3<T> tv0 = v3f<T>(ch.v0[j]);
+        const V3<T> tv1 = tv0 + v3f<T>(ch.e0[j]);
+        const V3<T> tv2 = tv0 + v3f<T>(ch.e1[j]);
+        const MD<T, 2> t = mdot(m3<T, 2>(tv0) - ro_j, m3<T, 2>(ng)) / mdot(m3<T, 2>(ng), rd_j);
+        const MD3<T, 2> p = ro_j + rd_j * t;
+        MD<T, 2> v = mdot(p - m3<T, 2>(tv1), m3<T, 2>(vcross(ng, tv1 - tv0)));
+        MD<T, 2> w = mdot(p - m3<T, 2>(tv2), m3<T, 2>(vcross(ng, tv2 - tv1)));
+        MD<T, 2> u = mdot(p - m3<T, 2>(tv0), m3<T, 2>(vcross(ng, tv0 - tv2)));
+        const MD<T, 2> area = u + v + w;
+        u = u / area;
+        v = v / area;
+        w = w / area;
+        const V3<T> n0 = v3f<T>(ch.n0[j]);
+        const V3<T> n1 = n0 + v3f<T>(ch.ne0[j]);
+        const V3<T> n2 = n0 + v3f<T>(ch.ne1[j]);
+        const MD3<T, 2> n = m3<T, 2>(n0) * w + m3<T, 2>(n1) * u + m3<T, 2>(n2) * v;
+        const MD3<T, 2> wi = -rd_j;
+        MD3<T, 2> wo;
+        auto refr = [](const MD3<T, 2>& wv, const MD3<T, 2>& nv, T e, bool& tir) {
+            const MD<T, 2> NoN = mdot(nv, nv), WIoN = mdot(wv, nv), WoW = mdot(wv, wv);
+            const MD<T, 2> kk = NoN * WoW * mconst<T, 2>(e * e - T(1)) + WIoN * WIoN;
+            tir = kk.v < T(0);
+            if (tir) return m3<T, 2>(v3<T>(0, 0, 0));
+            return -wv * NoN + nv * (WIoN - msqrt(kk));
+        };
+        if ((events >> j) & 1u) {
+            bool tir;
+            if (mdot(wi, n).v < T(0)) {
+                wo = refr(wi, -n, T(1) / eta, tir);
+                if (tir) return T(3.402823466e+38f);
+            } else {
+                wo = refr(wi, n, eta, tir);
+            }
+        } else {
+            wo = n * mdot(wi, n) * mconst<T, 2>(T(2)) / mdot(n, n) - wi;
+        }
+        ro_j = p;
+        rd_j = wo;
+    }
+    const V3<T> p_last = v3<T>(ro_j.x.v, ro_j.y.v, ro_j.z.v);
+    const MD3<T, 2> pn = m3<T, 2>(p_last - p_end);
+    const MD<T, 2> t = mdot(m3<T, 2>(p_end) - ro_j, pn) / mdot(pn, rd_j);
+    const MD3<T, 2> pf = ro_j + rd_j * t;
+    const V3<T> ax0 = v3<T>(pf.x.g[0], pf.y.g[0], pf.z.g[0]), ax1 = v3<T>(pf.x.g[1], pf.y.g[1], pf.z.g[1]);
+    const T len0 = vlength(ax0), len1 = vlength(ax1);
+    const T s = vlength(vcross(ax0 / len0, ax1 / len1));
+    return len0 * len1 * vfmax(s, T(0.01));
+}
+
+// position of the k-th (0-based) set bit of a 64-bit mask
+PZ_D int nth_bit64(unsigned long long m, int k)
+{
+    const uint32_t lo = (uint32_t)m;
+    const int c = __popc(lo);
+    if (k < c) return (int)__fns(lo, 0, k + 1);
+    return 32 + (int)__fns((uint32_t)(m >> 32), 0, k - c + 1);
+}
+
 }  // namespace batched
 }  // namespace pz

@@ -16,6 +16,7 @@ struct BatchArgs {
     unsigned long long* counters;      // device u64[10] diagnostics (see kCnt*), or null
     double polishDet;                  // FP64 polish below this relative det (<= 0: never)
     int continuation;                  // 1: refine predicted roots instead of solving from the photon start
+    float illDet;                      // relative det below which an item takes per-bin solves (near a fold)
 };
 
 // diagnostics counters

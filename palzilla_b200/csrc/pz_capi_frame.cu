@@ -247,6 +247,7 @@ extern "C" int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32
     b.counters = reinterpret_cast<unsigned long long*>(base + 64);
     b.polishDet = desc->polish_det < 0.0f ? 0.0 : (desc->polish_det == 0.0f ? 1.0e-6 : (double)desc->polish_det);
     b.continuation = desc->continuation;
+    b.illDet = desc->fold_det < 0.0f ? 0.0f : (desc->fold_det == 0.0f ? 1.0e-2f : desc->fold_det);
     if (desc->n_paths == 0) { clear_error(); return PZ_OK; }
     cudaError_t e = cudaMemsetAsync(base, 0, 256, S(stream));
     if (e == cudaSuccess) e = batched::launch_solve_batched(desc->K, b, blocks_per_sm > 0 ? blocks_per_sm : 2, S(stream));
