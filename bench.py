@@ -1,0 +1,482 @@
+"""Benchmark of the caustics hot path: specular paths solved per second and ms/frame of the
+batched persistent solver against the plain per-tuple solver, on the two-refraction
+dispersive sphere (icosphere subdivided 5 times = 20,480 triangles, r 0.5 at (0,1,0),
+Cauchy 1.5 + 4200/nm^2, 4x4 receiver, light at (0,4,0), 1024x1024, 64 wavelength bins,
+205 photons per triangle = 4.2M ~ 2^22 Sobol-seeded photons, event string TT).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one frame with the scene and its LBVH resident in HBM: eye pass, photon pass
+into the PathCache, lookup/flatten of (pixel, tuple) work items with the count read back,
+tuple-coherence sort and reorder, the batched solve of every item for all 64 bins, and the
+spectral resolve.  The unit is one (pixel, tuple, wavelength-bin) specular path solve,
+counted on the device.  The same frame is then rendered with the plain per-tuple solver
+(one thread per path and bin, the reference's kernel structure) for the speed-up and the
+relative RMSE between the two images.
+
+Under torchrun each rank renders its own replica of the frame (weak scaling, no data-path
+collective): value = all ranks' path solves / the slowest rank's device time.
+``--impl reference`` times the reference's own CPU solve (solveConstraints,
+contributableThroughput, dAdw, built from the reference sources into oracle/_ref) on the
+host cores over a bounded sample of the frame's work items, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "specular paths solved/s and ms/frame, batched vs plain GPU at 1e-3 image RMSE"
+UNIT = "paths/s"
+WORKLOAD = {
+    "workload": "two-refraction dispersive sphere",
+    "triangles": 20480, "scene": "icosphere-5 r=0.5 at (0,1,0), 4x4 receiver at y=0, light (0,4,0)",
+    "ior": "cauchy 1.5 + 4200/nm^2", "image": "1024x1024", "bins": 64, "lambda_nm": [380, 780],
+    "photons": 20480 * 205, "events": "TT", "path_cache": 1 << 22,
+    "l2": "no flush: every frame streams buffers larger than L2 (PathCache 252 MB, spectral image 268 MB)",
+}
+# kernels of this library launched per frame: k_primary, k_photon, k_lookup, sort k_hist + 4 x k_pass,
+# k_reorder, k_phase1, k_phase2, k_resolve_spectral
+LAUNCHES_PER_FRAME = 12
+# DRAM bytes per work item of k_phase1 + k_phase2 from the ncu capture of the solve (0: not captured)
+NCU_SOLVE_TRAFFIC_PER_ITEM = 0.0
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        threading.Thread(target=self._read, daemon=True).start()
+        time.sleep(0.3)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self) -> dict:
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        rows = [r for r in self.rows if len(r) >= 9]
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [v for v in (num(r[1]) for r in rows) if v is not None]
+        mx = [v for v in (num(r[2]) for r in rows) if v is not None]
+        reasons = sorted({self.NAMES[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# -------------------------------------------------------------------------------- ranks
+def setup_dist():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    import torch
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        torch.cuda.synchronize()
+
+
+def reduce(world, v: float, op: str) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def sphere():
+    from palzilla_b200 import scenes as S
+    sc = S.sphere_scene()
+    sc.photons_per_triangle = 205
+    return sc
+
+
+# -------------------------------------------------------------------------------- our arm
+class Renderer:
+    """One frame of the hot path on the current device (all buffers allocated up front)."""
+
+    def __init__(self, sc):
+        import torch
+        from palzilla_b200 import api as A
+        from palzilla_b200.scenes import event_descriptor
+        self.A, self.sc = A, sc
+        self.ds = A.DeviceScene(sc)
+        self.frame = A.Frame(sc, path_capacity=1 << 25)
+        self.cache = A.PathCache(capacity=1 << 22, step=sc.cell_step)
+        self.sorter = A.OnesweepSort()
+        self.scratch = A.Scratch()
+        self.ev = event_descriptor(sc.events)
+        self.etas = torch.from_numpy(sc.bin_etas()).cuda()
+        npx = sc.width * sc.height
+        self.spectral = torch.zeros((npx, sc.n_bins), device="cuda")
+        self.rgb = torch.zeros((npx, 4), device="cuda")
+        self.pixels = torch.zeros(npx, dtype=torch.int32, device="cuda")
+        self.stats = torch.zeros(3, dtype=torch.int64, device="cuda")
+        self.n_paths = 0
+
+    def prepare(self, iteration: int):
+        """Eye pass, photon pass, lookup/flatten (count read back), sort and reorder."""
+        A, fr = self.A, self.frame
+        A.solve_primary(self.ds, fr, iteration=iteration)
+        self.cache.clear()
+        A.photon_trace(self.ds, self.cache, iteration=iteration)
+        self.n_paths = A.lookup_flatten(fr, self.cache, self.ev)
+        A.sort_and_reorder(fr, self.n_paths, self.sorter)
+
+    def solve(self, plain: bool = False, exact: bool = False, solve_events=None):
+        """Specular solve of the prepared work list into a cleared spectral image, then resolve."""
+        A, sc = self.A, self.sc
+        self.spectral.zero_()
+        d = A.solve_desc(self.ds, self.frame, self.cache, sc.events, self.n_paths, spectral=self.spectral,
+                         etas=self.etas, stats=self.stats, exact=exact)
+        if solve_events:
+            solve_events[0].record()
+        if plain:
+            A.solve_specular_plain(d)
+        else:
+            A.solve_specular_batched(d, self.scratch)
+        if solve_events:
+            solve_events[1].record()
+        A.resolve_spectral(self.spectral, sc, rgb=self.rgb, pixels=self.pixels)
+
+    def frame_step(self, iteration: int, plain: bool = False, solve_events=None):
+        self.prepare(iteration)
+        self.solve(plain=plain, solve_events=solve_events)
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = setup_dist()
+    sc = sphere()
+    R = Renderer(sc)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    def timed_frames(k, first, plain):
+        """k frames bracketed by barriers; returns (device ms, path solves, solve-stage ms list)."""
+        solve = [(ev(), ev()) for _ in range(k)]
+        e0, e1 = ev(), ev()
+        R.stats.zero_()
+        barrier(world)
+        e0.record()
+        for i in range(k):
+            R.frame_step(first + i, plain=plain, solve_events=solve[i])
+        e1.record()
+        barrier(world)
+        return e0.elapsed_time(e1), float(R.stats[0].item()), [a.elapsed_time(b) for a, b in solve]
+
+    for i in range(args.warmup):
+        R.frame_step(i)
+    barrier(world)
+
+    # ---- timed batched frames, clocks sampled meanwhile
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms, paths, solve_ms = timed_frames(args.steps, 100, plain=False)
+    clk = clocks.stop()
+    t_max = reduce(world, ms, "max")
+    paths_all = reduce(world, paths, "sum")
+    value = paths_all / (t_max / 1e3)
+    counters = R.A.batched_counters(R.scratch)
+    n_items = R.n_paths
+    contributing = float(R.stats[2].item()) / args.steps
+
+    # ---- plain per-tuple solve of the same frames (fewer of them: it is several times slower)
+    kp = max(1, min(args.steps, args.plain_steps))
+    R.frame_step(100, plain=True)
+    p_ms, p_paths, p_solve_ms = timed_frames(kp, 100, plain=True)
+    p_tmax = reduce(world, p_ms, "max")
+    p_value = reduce(world, p_paths, "sum") / (p_tmax / 1e3)
+
+    # ---- image agreement on identical solver inputs (one PathCache and work list).  The photon
+    # pass itself is not deterministic: the first photon to claim a PathCache slot supplies the
+    # tuple's Newton start, as in the reference, so two frames of one iteration already differ.
+    def rel(a, b):
+        return float(torch.sqrt(((a - b).double() ** 2).mean()) / torch.sqrt((b.double() ** 2).mean()))
+    imgs = {}
+    for tag, plain, exact in (("plain_exact", True, True), ("plain", True, False), ("batched", False, False)):
+        R.solve(plain=plain, exact=exact)
+        torch.cuda.synchronize()
+        imgs[tag] = (R.spectral.clone(), R.rgb[:, :3].clone())
+    rmse = {}
+    for a, b in (("batched", "plain_exact"), ("batched", "plain"), ("plain", "plain_exact")):
+        rmse[f"{a}_vs_{b}"] = {"spectral": rel(imgs[a][0], imgs[b][0]), "rgb": rel(imgs[a][1], imgs[b][1])}
+    del imgs
+
+    # ---- end to end through the C ABI: pinned host scene -> HBM, LBVH build, frame, RGBA8 image -> host
+    tris_h = torch.from_numpy(np.ascontiguousarray(sc.tris)).pin_memory()
+    att_h = torch.from_numpy(np.ascontiguousarray(sc.attribs).view(np.uint8)).pin_memory()
+    img_h = torch.empty(sc.width * sc.height, dtype=torch.int32).pin_memory()
+    ke = max(1, min(args.steps, 3))
+    e0, e1 = ev(), ev()
+    R.stats.zero_()
+    barrier(world)
+    e0.record()
+    for i in range(ke):
+        R.ds.tris.copy_(tris_h, non_blocking=True)
+        R.ds.attribs.copy_(att_h, non_blocking=True)
+        R.ds.builder.build(R.ds.tris, R.ds.n, 0)
+        R.frame_step(200 + i)
+        img_h.copy_(R.pixels, non_blocking=True)
+    e1.record()
+    barrier(world)
+    e2e_ms = reduce(world, e0.elapsed_time(e1), "max")
+    e2e_paths = reduce(world, float(R.stats[0].item()), "sum")
+
+    # ---- roofline of the dominant kernel pair (the batched solve)
+    hbm, hbm_kind = peaks()
+    solve_avg = float(np.mean(solve_ms))
+    # algorithmic bytes per work item: SpecularPath 8 + FirstDiffuse 40 + PathCache tuple 16 + params 32
+    # + two triangles 72 + two attributes 80 = 248 B read once; 4 B per contributing (item, bin) added
+    alg_bytes = n_items * 248.0 + contributing * 4.0
+    achieved = alg_bytes / (solve_avg / 1e3) / 1e9
+    roofline = {"kernel": "k_phase1 + k_phase2 (batched solve)", "bound": "hbm", "achieved": achieved, "peak": hbm,
+                "unit": "GB/s", "frac": achieved / hbm, "peak_kind": hbm_kind,
+                "traffic": NCU_SOLVE_TRAFFIC_PER_ITEM * n_items if NCU_SOLVE_TRAFFIC_PER_ITEM else None,
+                "algorithmic_bytes": alg_bytes,
+                "note": "issue-bound (FP32 Newton/QR and BVH visibility in registers): the HBM fraction is "
+                        "small by design; SM issue and occupancy are in profiles/"}
+
+    sort_build = bench_sort_build(hbm, hbm_kind) if (rank == 0 and not args.no_sort) else None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(R, seconds=args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(WORKLOAD, parallelism=f"{world} independent frame replicas" if world > 1 else "1 GPU"),
+            "ms_per_frame": t_max / args.steps,
+            "work_items_per_frame": n_items,
+            "path_solves_per_frame": paths / args.steps,
+            "solve_ms_per_frame": solve_avg,
+            "plain": {"value": p_value, "ms_per_frame": p_tmax / kp, "solve_ms_per_frame": float(np.mean(p_solve_ms)),
+                      "steps": kp},
+            "speedup_paths_per_s_vs_plain": value / p_value,
+            "speedup_solve_vs_plain": float(np.mean(p_solve_ms)) / solve_avg,
+            "image_rel_rmse": rmse,
+            "batched_counters": counters,
+            "e2e": {"value": e2e_paths / (e2e_ms / 1e3), "unit": UNIT, "steps": ke, "ms_per_step": e2e_ms / ke,
+                    "h2d_bytes_per_step": int(tris_h.numel() * 4 + att_h.numel()),
+                    "d2h_bytes_per_step": int(img_h.numel() * 4),
+                    "path": "pinned host scene -> device, pz_bvh_build, full frame, RGBA8 image -> pinned host"},
+            "gpu_launches": LAUNCHES_PER_FRAME * args.steps,
+            "roofline": roofline,
+            "sort_build": sort_build,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def bench_sort_build(hbm, hbm_kind, n=1 << 24):
+    """Onesweep sort of n {32-bit key, 32-bit index} pairs and the LBVH build of n random
+    triangles (the sort + build workload at its largest size), L2 flushed between reps."""
+    import torch
+    from palzilla_b200 import scenes as S
+    from palzilla_b200.api import BVHGPUBuilder, OnesweepSort
+    g = torch.Generator(device="cuda").manual_seed(1)
+    base = torch.randint(0, 1 << 30, (n,), device="cuda", generator=g, dtype=torch.int64) | \
+        (torch.arange(n, device="cuda", dtype=torch.int64) << 32)
+    keys, tmp = base.clone(), torch.empty_like(base)
+    sorter = OnesweepSort()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def med(fn, reps=7, warm=3):
+        ts = []
+        for i in range(warm + reps):
+            keys.copy_(base)
+            flush.fill_(i & 0xFF)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            if i >= warm:
+                ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+    sort_ms = med(lambda: sorter.sort(keys, None, tmp, None, n, 0, 32))
+    tris = torch.from_numpy(S.random_soup(n, seed=1001)).cuda()
+    b = BVHGPUBuilder()
+    build_ms = med(lambda: b.build(tris, n, 0))
+    sort_gbs = 72.0 * n / (sort_ms / 1e3) / 1e9
+    build_gbs = (189.0 + 72.0) * n / (build_ms / 1e3) / 1e9
+    return {"n": n, "sort_ms": sort_ms, "keys_per_s": n / (sort_ms / 1e3),
+            "sort_roofline": {"bound": "hbm", "achieved": sort_gbs, "peak": hbm, "unit": "GB/s",
+                              "frac": sort_gbs / hbm, "peak_kind": hbm_kind, "bytes_per_key": 72},
+            "build_ms": build_ms, "triangles_per_s": n / (build_ms / 1e3),
+            "build_roofline": {"bound": "hbm", "achieved": build_gbs, "peak": hbm, "unit": "GB/s",
+                               "frac": build_gbs / hbm, "peak_kind": hbm_kind, "bytes_per_triangle": 261}}
+
+
+# -------------------------------------------------------------------------------- CPU
+def _cpu_lib():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    ref = O.reference()
+    return (ref, "reference") if ref is not None else (O.oracle(), "port")
+
+
+def _sample(pairs, n, seed):
+    rng = np.random.default_rng(seed)
+    return pairs[np.sort(rng.choice(len(pairs), size=min(n, len(pairs)), replace=False))].copy()
+
+
+def cpu_baseline(R, seconds=15.0):
+    """The reference's CPU solve over a bounded sample of this frame's work items, OpenMP
+    over all host threads; about `seconds` of CPU work."""
+    lib, kind = _cpu_lib()
+    import oracle as O
+    sc = R.sc
+    n = R.n_paths
+    pairs = R.frame.paths[: n * 8].cpu().numpy().view(np.int32).reshape(-1, 2)
+    cache = R.cache.to_host()
+    fd = R.frame.fd.cpu().numpy().view(np.float32).reshape(-1, 10)
+    nodes = np.frombuffer(R.ds.internals[: (R.ds.n - 1) * 64].cpu().numpy().tobytes(), O.NODE_DTYPE)
+    bvh = {"nodes": nodes, "root": R.ds.builder.root}
+    etas = sc.bin_etas()
+    probe = _sample(pairs, 512, 1)
+    t0 = time.perf_counter()
+    lib.render_pairs(2, probe, cache, fd, bvh, sc, etas)
+    dt = time.perf_counter() - t0
+    m = int(min(len(pairs), max(512, len(probe) * seconds / max(dt, 1e-3))))
+    sel = _sample(pairs, m, 2)
+    t0 = time.perf_counter()
+    _, st = lib.render_pairs(2, sel, cache, fd, bvh, sc, etas)
+    dt = time.perf_counter() - t0
+    return {"value": float(st[0]) / dt, "unit": UNIT, "cores": lib.max_threads(), "kind": kind,
+            "sample": f"solve stage only: {len(sel)} of the frame's {n} (pixel, tuple) work items x 64 bins "
+                      f"= {int(st[0])} path solves in {dt:.1f} s"}
+
+
+def run_reference(args):
+    """The reference's own CPU implementation of the path on the host cores (rank 0 only):
+    LBVH, photon pass, PathCache and work list are built once on the CPU; each step solves
+    a bounded random sample of the frame's work items for all 64 bins."""
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from palzilla_b200.scenes import event_descriptor
+    lib, kind = _cpu_lib()
+    orc = O.oracle()
+    sc = sphere()
+    b = lib.build_bvh(sc.tris)
+    bvh = {"nodes": b["nodes"], "root": int(np.asarray(b["root"]).ravel()[0])}
+    recs = lib.photon_trace(bvh, sc, iteration=0)
+    cache = lib.cache_build(recs, capacity=1 << 22, step=sc.cell_step)
+    cam = sc.camera
+    gen = orc.lookat(cam.eye, cam.center, cam.up, cam.fovy, sc.width, sc.height)
+    _, fd = orc.solve_primary(bvh, sc, gen, iteration=0)
+    valid = (fd[:, 6:9] != 0).any(1).astype(np.uint8)
+    _, pairs = orc.lookup_flatten(cache, fd[:, 0:3], valid, event_descriptor(sc.events), pair_cap=1 << 25)
+    etas = sc.bin_etas()
+    times, solves = [], []
+    for i in range(args.warmup + args.steps):
+        sel = _sample(pairs, args.ref_items, 10 + i)
+        t0 = time.perf_counter()
+        _, st = lib.render_pairs(2, sel, cache, fd, bvh, sc, etas)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+            solves.append(float(st[0]))
+    value = sum(solves) / sum(times)
+    sample = (f"solve stage only: {min(args.ref_items, len(pairs))} random (pixel, tuple) work items x 64 bins "
+              f"per step from the CPU-built frame's {len(pairs)} work items")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(WORKLOAD, parallelism="host cores"),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": lib.max_threads(), "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--plain-steps", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-items", type=int, default=20000)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-sort", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -507,7 +507,16 @@ static cudaError_t launch_k(const BatchArgs& a, int blocksPerSM, cudaStream_t s)
     return cudaGetLastError();
 }
 
-size_t record_bytes(int K) { return (size_t)(24 + 16 * K + 8 * (K & 1)); }
+size_t record_bytes(int K)
+{
+    switch (K) {
+        case 1: return sizeof(PairRec<1>);
+        case 2: return sizeof(PairRec<2>);
+        case 3: return sizeof(PairRec<3>);
+        case 4: return sizeof(PairRec<4>);
+        default: return 0;
+    }
+}
 
 cudaError_t launch_solve_batched(int K, const BatchArgs& a, int blocksPerSM, cudaStream_t s)
 {

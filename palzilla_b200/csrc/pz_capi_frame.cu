@@ -242,7 +242,7 @@ extern "C" int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32
     b.workCounter = reinterpret_cast<unsigned long long*>(base + 8);
     b.recordCount = reinterpret_cast<unsigned long long*>(base + 16);
     b.records = base + 256;
-    b.recordCapacity = desc->n_paths;
+    b.recordCapacity = (scratch_bytes - 256) / batched::record_bytes(desc->K);
     b.nPathsDev = n_paths_dev;
     b.counters = reinterpret_cast<unsigned long long*>(base + 64);
     b.polishDet = desc->polish_det < 0.0f ? 0.0 : (desc->polish_det == 0.0f ? 1.0e-6 : (double)desc->polish_det);
