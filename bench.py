@@ -47,8 +47,9 @@ WORKLOAD = {
 # kernels of this library launched per frame: k_primary, k_photon, k_lookup, sort k_hist + 4 x k_pass,
 # k_reorder, k_phase1, k_phase2, k_resolve_spectral
 LAUNCHES_PER_FRAME = 12
-# DRAM bytes per work item of k_phase1 + k_phase2 from the ncu capture of the solve (0: not captured)
-NCU_SOLVE_TRAFFIC_PER_ITEM = 0.0
+# DRAM bytes (read + write) per work item of k_phase1 + k_phase2, from one ncu capture of the
+# first frame of this workload (profiles/sphere_solver_photon_kernels.md): 3411.8 MB / 19.8 M items
+NCU_SOLVE_TRAFFIC_PER_ITEM = 172.3
 
 
 def peaks():
@@ -374,6 +375,19 @@ def bench_sort_build(hbm, hbm_kind, n=1 << 24):
                                "frac": build_gbs / hbm, "peak_kind": hbm_kind, "bytes_per_triangle": 261}}
 
 
+def run_sort_build(args):
+    """Sort + build alone: n uniform random triangles (edges of 1e-3 to 1e-2), 32-bit Morton
+    keys with 32-bit index payloads, onesweep sort and LBVH build, one line per size."""
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    hbm, hbm_kind = peaks()
+    for lg in [int(x) for x in args.sizes.split(",") if x]:
+        r = bench_sort_build(hbm, hbm_kind, n=1 << lg)
+        print(json.dumps({"metric": "keys/s and LBVH build ms (onesweep sort + build)", "workload": "sort_build",
+                          "value": r["keys_per_s"], "unit": "keys/s", "higher_is_better": True,
+                          "dtype": "u64 (32-bit key + 32-bit index)", "data": "synthetic", **r}), flush=True)
+
+
 # -------------------------------------------------------------------------------- CPU
 def _cpu_lib():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -471,8 +485,13 @@ def main():
     ap.add_argument("--ref-items", type=int, default=20000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-sort", action="store_true")
+    ap.add_argument("--workload", default="sphere", choices=["sphere", "sort_build"],
+                    help="sphere: the frame benchmark; sort_build: onesweep sort + LBVH build alone")
+    ap.add_argument("--sizes", default="20,22,24", help="log2 sizes of the sort_build workload")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.workload == "sort_build":
+        run_sort_build(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
