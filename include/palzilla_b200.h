@@ -88,6 +88,22 @@ PZ_API int pz_onesweep_sort(void* keys_dev, uint32_t* values_dev, void* tmp_keys
                      int key_bytes, int start_bit, int end_bit, void* scratch_dev, size_t scratch_bytes,
                      pz_stream_t stream);
 
+/* No reference counterpart (the reference's OnesweepSort owns and allocates its scratch).
+ * The same sort as pz_onesweep_sort, with the scratch taken from a static device array of
+ * this library (2,113,536 bytes per device: the 16 KiB header and look-back rows for
+ * PZ_ONESWEEP_STATIC_MAX_KEYS keys), for callers that cannot allocate device memory at call
+ * time.  n > PZ_ONESWEEP_STATIC_MAX_KEYS is rejected with PZ_ERR_SCRATCH_TOO_SMALL before
+ * any device work.  The first call on a device looks up the array's address (and may load
+ * the module), so make it before any stream capture.  Nothing has to be zeroed by the
+ * caller: each call clears what it uses on `stream`.  All calls on one device share the
+ * array: calls whose GPU work can overlap (unordered streams) race; order them on one
+ * stream.  When status_dev != NULL the sort's status word (PZ_DEVICE_ERR_* bits, 0 = ok)
+ * is copied there on `stream` after the sort. */
+#define PZ_ONESWEEP_STATIC_MAX_KEYS (1u << 22)
+PZ_API int pz_onesweep_sort_static(void* keys_dev, uint32_t* values_dev, void* tmp_keys_dev, uint32_t* tmp_values_dev,
+                            uint32_t n, int key_bytes, int start_bit, int end_bit, uint32_t* status_dev,
+                            pz_stream_t stream);
+
 /* ---------------------------------------------------------------- LBVH build
  * Replaces minimum_lbvh::BVHGPUBuilder::build (minimum_lbvh.h:798-886):
  * scene AABB, 32-bit Morton keys (upper 32 bits of a 63-bit code), stable radix

@@ -55,6 +55,7 @@ SIGNATURES = {
     "pz_scratch_status": (i32, [vp, C.POINTER(u32), vp]),
     "pz_onesweep_scratch_bytes": (sz, [u32]),
     "pz_onesweep_sort": (i32, [vp, vp, vp, vp, u32, i32, i32, i32, vp, sz, vp]),
+    "pz_onesweep_sort_static": (i32, [vp, vp, vp, vp, u32, i32, i32, i32, vp, vp]),
     "pz_bvh_scratch_bytes": (sz, [i32]),
     "pz_bvh_build": (i32, [vp, i32, u32, vp, vp, vp, sz, vp]),
     "pz_bvh_debug_views": (i32, [vp, i32, C.POINTER(vp), C.POINTER(vp), vp, vp]),

@@ -36,6 +36,7 @@ UNITS = {
     "pz_batched": ("pz_batched.cu", []),
     "pz_capi": ("pz_capi.cu", []),
     "pz_capi_frame": ("pz_capi_frame.cu", []),
+    "pz_sort_static": ("pz_sort_static.cu", []),
 }
 
 
