@@ -45,8 +45,8 @@ WORKLOAD = {
     "l2": "no flush: every frame streams buffers larger than L2 (PathCache 252 MB, spectral image 268 MB)",
 }
 # kernels of this library launched per frame: k_primary, k_photon, k_lookup, sort k_hist + 4 x k_pass,
-# k_reorder, k_phase1, k_phase2, k_resolve_spectral
-LAUNCHES_PER_FRAME = 12
+# k_reorder, k_probe, k_phase1, k_phase2, k_resolve_spectral
+LAUNCHES_PER_FRAME = 13
 # DRAM bytes (read + write) per work item of k_phase1 + k_phase2, from one ncu capture of the
 # first frame of this workload (profiles/sphere_solver_photon_kernels.md): 3411.8 MB / 19.8 M items
 NCU_SOLVE_TRAFFIC_PER_ITEM = 172.3

@@ -224,7 +224,9 @@ typedef struct pz_solve_desc {
     unsigned long long* stats;             /* device u64[3]: items solved, converged, contributing (or NULL) */
     int exact_arithmetic;                  /* plain solve: 1 = no FMA contraction (bit-compatible with the CPU oracle) */
     float polish_det;                      /* batched solve: FP64 polish of roots whose relative determinant
-                                              prod|R_ii| / max|R_ii|^(2K) is below this; 0 = 1e-6, < 0 = never */
+                                              prod|R_ii| / max|R_ii|^(2K) is below this; <= 0 = never (the
+                                              default: the image then follows the reference's float
+                                              arithmetic); 1e-6 polishes near-singular Jacobians */
     int continuation;                      /* batched solve: 1 = refine each bin from its predicted root
                                               (faster; roots near triangle edges are accepted more often
                                               than the reference's Newton path accepts them) */

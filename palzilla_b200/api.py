@@ -312,11 +312,11 @@ def solve_specular_batched(desc, scratch: Scratch, n_paths_dev=None, blocks_per_
 
 
 BATCH_COUNTERS = ("skipped", "predicted", "fallback", "newton_bins", "fp64_polish", "vis_overflow", "vis_candidates",
-                  "vis_queries", "fallback_noconv", "fallback_shift")
+                  "vis_queries", "fallback_noconv", "fallback_shift", "fallback_probe")
 
 
 def batched_counters(scratch: Scratch) -> dict:
-    v = scratch.buf[64:144].view(torch.int64).cpu().tolist()
+    v = scratch.buf[64:64 + 8 * len(BATCH_COUNTERS)].view(torch.int64).cpu().tolist()
     return dict(zip(BATCH_COUNTERS, v))
 
 

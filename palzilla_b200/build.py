@@ -33,7 +33,7 @@ UNITS = {
     "pz_frame": ("pz_frame.cu", ["-fmad=false"]),
     "pz_solve": ("pz_solve.cu", []),
     "pz_solve_exact": ("pz_solve.cu", ["-fmad=false", "-DPZ_SOLVE_EXACT"]),
-    "pz_batched": ("pz_batched.cu", []),
+    "pz_batched": ("pz_batched.cu", ["-fmad=false"]),
     "pz_capi": ("pz_capi.cu", []),
     "pz_capi_frame": ("pz_capi_frame.cu", []),
     "pz_sort_static": ("pz_sort_static.cu", []),

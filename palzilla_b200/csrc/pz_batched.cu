@@ -1,29 +1,31 @@
 // pz_batched.cu -- batched persistent specular solver (binned wavelengths).
 //
 // Same work items and results as the plain solver (one (pixel, tuple) work item solved
-// for every wavelength bin, solveSpecularPath<K> semantics per bin), organised for the
-// GPU:
-//  * persistent warps pull chunks of 32 work items from a device counter (no host
-//    round trip: the item count is read from device memory);
-//  * phase 1, one lane per item: an unconstrained Newton solve at the centre bin from
-//    the photon's barycentrics, and the derivative of the root with respect to eta from
-//    the same Jacobian (implicit-function theorem).  The root of every other bin is
-//    predicted linearly; bins whose predicted root lies outside the triangles by more
-//    than kMargin are rejected without a solve, the rest are refined in phase 2.  Items
-//    whose centre solve does not converge, or whose prediction is unreliable, fall back
-//    to the plain per-bin solve from the photon's barycentrics;
-//  * phase 2, one lane per bin: Newton with the reference's rules (multi-tangent duals:
-//    one pass per iteration) from the photon's barycentrics, as the plain solver -- the
-//    reference's accept/reject decision depends on the Newton path through its
-//    shrinking edge test, so this keeps it -- or, with continuation enabled, from the
-//    predicted root (fewer iterations, roots near triangle edges accepted more
-//    often than the reference does); admissibility checks, then
-//    visibility shared by the whole warp: for each path segment one BVH query with the
-//    segment fattened to cover every bin's segment collects the few candidate
-//    triangles, and each bin tests only those (exact: a triangle that cuts any bin's
-//    segment lies within the fattening radius of the reference segment);
-//  * FP64 polish: bins of items with |det R| < 1e-6 at the root (ill-conditioned) are
-//    re-solved and re-checked in double precision from the FP32 root.
+// for every wavelength bin with solveSpecularPath<K> semantics, pk.h / main_gpu.cu:418-497),
+// organised for the GPU in three launches:
+//  * k_probe, one thread per (item, probe bin): the plain path's solve from the photon's
+//    barycentrics at the centre, first and last bin;
+//  * k_phase1, one thread per item: the branch of roots through the centre bin (the probe's
+//    root, or an unconstrained Newton solve from the photon's barycentrics), its
+//    derivative in eta from the same Jacobian (implicit-function theorem), the two end-bin
+//    roots refined from the tangent prediction, and a quadratic prediction of every bin's
+//    root.  Bins whose predicted root lies outside a triangle by more than the prediction
+//    error (plus the bin next to each edge crossing) need no solve; an item with no bin
+//    left is skipped.  Items whose branch disagrees with a probe (the plain path reaches
+//    another root there, or rejects where the branch is deep inside), whose solves did not
+//    converge, whose prediction is strongly nonlinear, or whose Jacobian is near a fold,
+//    take the plain per-bin solve for every bin.  Items with work are appended to a record
+//    list with warp-aggregated atomics;
+//  * k_phase2, persistent, one warp per record and one lane per bin: bins deep inside the
+//    triangles refine the predicted root; every other bin runs the plain path's solve from
+//    the photon's barycentrics, so its accept / reject decision is the plain one.  Then
+//    admissibility, visibility shared by the whole warp (one BVH query per path segment
+//    with the segment fattened to cover every bin's segment; each bin tests only those
+//    candidates), dAdw and the spectral accumulation.  Optional FP64 polish of roots whose
+//    relative Jacobian determinant is below a threshold.
+// The unit is compiled without FMA contraction: with the reference's operation order in
+// every Newton step, the image equals the reference's float arithmetic up to the order
+// of the float atomics.
 #include "pz_batched.cuh"
 #include "pz_batched_api.cuh"
 
@@ -44,6 +46,7 @@ constexpr int kWarpsPerBlock = 8;
 constexpr int kMaxCand = 32;
 constexpr float kMaxShift = 0.5f;    // a larger predicted shift over the band falls back
 constexpr float kDeep = 0.3f;        // a predicted root this far inside every triangle is refined, not re-solved
+constexpr float kProbeTol = 1.0e-3f;  // a plain-solve root farther than this from the followed branch is another root
 
 // Phase-1 result of one work item that has bins to refine (global, compacted).
 template <int K> struct PairRec {
@@ -52,6 +55,12 @@ template <int K> struct PairRec {
     unsigned long long mask;  // bins to solve (mode 1)
     unsigned long long warm;  // of those, bins whose root is deep inside: refine the prediction
     float xa[2 * K], xc[2 * K], xb[2 * K];  // roots at the first, centre and last bin
+};
+
+// The plain path's solve of one work item at one probe bin (q = 0: centre, 1: first, 2: last).
+template <int K> struct Probe {
+    float x[2 * K];
+    uint32_t ok;
 };
 
 // Quadratic (Lagrange) prediction of the root at eta from the roots at eta_a, eta_c, eta_b.
@@ -229,6 +238,56 @@ __device__ __noinline__ float dadw_out_of_line(const Chain<K>& ch, const float* 
 #endif
 }
 
+// The plain path's solve (solveConstraints' rules from the photon's start: cost tolerance,
+// edge rejection after the warm-up iterations) on the multi-tangent Jacobian, whose
+// columns follow the reference's single-tangent operation order.  Out of line: phase 2
+// calls it for every bin that is not refined from a prediction.
+template <int K>
+__device__ __noinline__ bool plain_solve(float* x, const Chain<K>& ch, float3 p_light, float3 p, float eta,
+                                         uint32_t events, int maxIterations, float tol, int warmup)
+{
+    int it;
+    float det;
+    return newton<float, K>(x, v3f<float>(p_light), v3f<float>(p), ch, eta, events, maxIterations, tol, warmup, true,
+                            &it, &det, 0);
+}
+
+// ---------------------------------------------------------------- probes
+// One thread per (work item, probe bin): the plain path's solver from the photon's start at
+// the centre, first and last bin.  Kept apart from phase 1 so that it runs at the plain
+// kernel's occupancy; the three probes of an item sit in adjacent threads.
+template <int K>
+__global__ void __launch_bounds__(256) k_probe(BatchArgs a)
+{
+    const int B = a.s.nBins;
+    const uint64_t nPaths = a.nPathsDev ? min((uint64_t)*a.nPathsDev, a.s.nPaths) : a.s.nPaths;
+    auto* probes = reinterpret_cast<Probe<K>*>(a.probes);
+    const V3<float> L = v3f<float>(a.s.p_light);
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < 3 * nPaths;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t idx = t / 3;
+        const int q = (int)(t - 3 * idx);
+        const SpecularPath sp = a.s.paths[idx];
+        const int4 ti = a.s.cache.tris[sp.cacheIndex];
+        const int tix[4] = {ti.x, ti.y, ti.z, ti.w};
+        Chain<K> ch;
+        load_chain<K>(ch, a.s.tris, a.s.attribs, tix);
+        const float4 q0 = a.s.cache.params[2 * sp.cacheIndex], q1 = a.s.cache.params[2 * sp.cacheIndex + 1];
+        const float pp[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+        Probe<K> r;
+#pragma unroll
+        for (int i = 0; i < 2 * K; i++) r.x[i] = pp[i];
+        const int b = q == 0 ? B / 2 : (q == 1 ? 0 : B - 1);
+        int it;
+        float det;
+        r.ok = newton<float, K>(r.x, L, v3f<float>(a.s.fds[sp.pixel].p), ch, a.s.etas[b], a.s.events,
+                                a.s.maxIterations, a.s.costTolerance, a.s.earlyTermWarmUp, true, &it, &det, 0)
+                   ? 1u
+                   : 0u;
+        probes[t] = r;
+    }
+}
+
 // ---------------------------------------------------------------- phase 1
 template <int K>
 __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
@@ -249,13 +308,25 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
         load_chain<K>(ch, a.s.tris, a.s.attribs, tix);
         const float4 q0 = a.s.cache.params[2 * sp.cacheIndex], q1 = a.s.cache.params[2 * sp.cacheIndex + 1];
         const float pp[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-        float x[2 * K];
+        float x[2 * K], xpc[2 * K];
 #pragma unroll
-        for (int i = 0; i < 2 * K; i++) x[i] = pp[i];
+        for (int i = 0; i < 2 * K; i++) x[i] = xpc[i] = pp[i];
         const V3<float> p = v3f<float>(a.s.fds[sp.pixel].p);
         int it;
-        float det;
-        const bool conv = newton<float, K>(x, L, p, ch, eta_c, a.s.events, 24, a.s.costTolerance, 0, false, &it, &det);
+        float det = 1.0f;
+        // the plain path's decision at the centre bin (k_probe); when it converged, its root
+        // is the branch followed below
+        const auto* pr = reinterpret_cast<const Probe<K>*>(a.probes) + 3 * idx;
+        const bool okc = pr[0].ok != 0;
+#pragma unroll
+        for (int i = 0; i < 2 * K; i++) xpc[i] = pr[0].x[i];
+        bool conv = okc;
+        if (okc) {
+#pragma unroll
+            for (int i = 0; i < 2 * K; i++) x[i] = xpc[i];
+        } else {
+            conv = newton<float, K>(x, L, p, ch, eta_c, a.s.events, 24, a.s.costTolerance, 0, false, &it, &det);
+        }
         PairRec<K> r;
         r.pixel = sp.pixel;
         r.slot = sp.cacheIndex;
@@ -263,7 +334,7 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
         r.polish = 0;
         r.mask = 0;
         r.warm = 0;
-        bool conv2 = false;
+        bool conv2 = false, probeFallback = false;
         if (conv && B >= 3) {
             // root derivative in eta at the centre (implicit-function theorem) and the two
             // end-bin roots, warm-started from the tangent prediction
@@ -320,15 +391,49 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
                     if (depth > -err) mask |= 1ull << b;
                     if (depth > kDeep + err) warm |= 1ull << b;
                 }
+                // the bin next to each end of a contributing run is solved too: that is where a
+                // root crosses a triangle edge, and where the prediction error matters most
+                const unsigned long long all = B == 64 ? ~0ull : ((1ull << B) - 1ull);
+                mask = (mask | (mask << 1) | (mask >> 1)) & all;
                 r.mask = mask;
                 r.warm = warm;
                 r.mode = mask ? 1 : 0;
+                // The plain path solves every bin from the photon's start, so its root can lie on
+                // another branch than the one followed here.  Probe the plain solve at the
+                // centre and both end bins: a converged root away from the followed branch, or a
+                // rejection where the branch is deep inside, sends the item to per-bin plain solves.
+                bool mismatch = false;
+#pragma unroll 1
+                for (int q = 0; q < 3 && !mismatch; q++) {
+                    const int b = q == 0 ? bc : (q == 1 ? 0 : B - 1);
+                    const float* xt = q == 0 ? r.xc : (q == 1 ? r.xa : r.xb);
+                    float xq[2 * K];
+                    const bool okq = pr[q].ok != 0;
+#pragma unroll
+                    for (int i = 0; i < 2 * K; i++) xq[i] = pr[q].x[i];
+                    if (okq) {
+                        float dev = 0.0f;
+#pragma unroll
+                        for (int i = 0; i < 2 * K; i++) dev = fmaxf(dev, fabsf(xq[i] - xt[i]));
+                        mismatch = !(dev < kProbeTol);
+                    } else {
+                        mismatch = ((warm >> b) & 1ull) != 0;
+                    }
+                }
+                if (mismatch) {
+                    probeFallback = true;
+                    r.mode = 2;
+                    r.mask = 0;
+                    r.warm = 0;
+                    if (a.counters) atomicAdd(a.counters + kCntFallbackProbe, 1ull);
+                }
             }
         }
         nItems += (unsigned long long)B;
         if (a.counters) {
             atomicAdd(a.counters + r.mode, 1ull);
-            if (r.mode == 2) atomicAdd(a.counters + (conv && conv2 ? kCntFallbackShift : kCntFallbackNoConv), 1ull);
+            if (r.mode == 2 && !probeFallback)
+                atomicAdd(a.counters + (conv && conv2 ? kCntFallbackShift : kCntFallbackNoConv), 1ull);
         }
         // warp-aggregated append of the items that have work
         const bool keep = r.mode != 0;
@@ -408,10 +513,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
                     for (int i = 0; i < 2 * K; i++) xs[i] = x0[i];
                 }
                 int it;
-                float det;
-                const bool conv = newton<float, K>(xs, L, p, ch, eta, a.s.events, a.s.maxIterations,
-                                                   a.s.costTolerance, a.s.earlyTermWarmUp, true, &it, &det,
-                                                   warm ? 1 : 0);
+                float det = 1.0f;
+                // a predicted root is refined by Newton; every other bin runs the plain path's
+                // solver from the photon's start, so its accept / reject decision is the plain one
+                const bool conv = warm ? newton<float, K>(xs, L, p, ch, eta, a.s.events, a.s.maxIterations,
+                                                          a.s.costTolerance, a.s.earlyTermWarmUp, true, &it, &det, 1)
+                                       : plain_solve<K>(xs, ch, a.s.p_light, fd.p, eta, a.s.events, a.s.maxIterations,
+                                                        a.s.costTolerance, a.s.earlyTermWarmUp);
                 if (a.counters) atomicAdd(a.counters + kCntNewton2, 1ull);
                 if (conv) {
                     nConv++;
@@ -502,9 +610,21 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
 template <int K>
 static cudaError_t launch_k(const BatchArgs& a, int blocksPerSM, cudaStream_t s)
 {
+    k_probe<K><<<kNumSMs * 16, 256, 0, s>>>(a);
     k_phase1<K><<<kNumSMs * 8, 256, 0, s>>>(a);
     k_phase2<K><<<kNumSMs * blocksPerSM, kWarpsPerBlock * 32, 0, s>>>(a);
     return cudaGetLastError();
+}
+
+size_t probe_bytes(int K)
+{
+    switch (K) {
+        case 1: return sizeof(Probe<1>);
+        case 2: return sizeof(Probe<2>);
+        case 3: return sizeof(Probe<3>);
+        case 4: return sizeof(Probe<4>);
+        default: return 0;
+    }
 }
 
 size_t record_bytes(int K)

@@ -220,7 +220,8 @@ extern "C" int pz_solve_specular_plain(const pz_solve_desc* desc, pz_stream_t st
 extern "C" size_t pz_solve_batched_scratch_bytes(int K, uint64_t max_paths)
 {
     if (K < 1 || K > 4) return 0;
-    return 256 + (size_t)max_paths * batched::record_bytes(K);
+    // header | one phase-1 record per work item | three plain-solve probes per work item
+    return 256 + (size_t)max_paths * (batched::record_bytes(K) + 3 * batched::probe_bytes(K));
 }
 
 extern "C" int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32_t* n_paths_dev, void* scratch_dev,
@@ -242,10 +243,12 @@ extern "C" int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32
     b.workCounter = reinterpret_cast<unsigned long long*>(base + 8);
     b.recordCount = reinterpret_cast<unsigned long long*>(base + 16);
     b.records = base + 256;
-    b.recordCapacity = (scratch_bytes - 256) / batched::record_bytes(desc->K);
+    b.recordCapacity = desc->n_paths;
+    b.probes = base + 256 + (size_t)desc->n_paths * batched::record_bytes(desc->K);
     b.nPathsDev = n_paths_dev;
+    static_assert(64 + 8 * batched::kNumCounters <= 256, "counters live in the 256-byte scratch header");
     b.counters = reinterpret_cast<unsigned long long*>(base + 64);
-    b.polishDet = desc->polish_det < 0.0f ? 0.0 : (desc->polish_det == 0.0f ? 1.0e-6 : (double)desc->polish_det);
+    b.polishDet = desc->polish_det > 0.0f ? (double)desc->polish_det : 0.0;
     b.continuation = desc->continuation;
     b.illDet = desc->fold_det < 0.0f ? 0.0f : (desc->fold_det == 0.0f ? 1.0e-2f : desc->fold_det);
     if (desc->n_paths == 0) { clear_error(); return PZ_OK; }

@@ -1,0 +1,174 @@
+"""Batched persistent solver (pz_solve_specular_batched) against the plain per-tuple solver
+and the CPU oracle, on identical solver inputs (one PathCache and one work list).
+
+The batched solver runs the reference's arithmetic without FMA contraction, as the
+exact-arithmetic plain build does, so its image equals the float oracle's (the reference's
+own CPU code) up to the order of the float atomics: relative RMSE <= 1e-5.  Against the
+plain FMA build it differs exactly as much as that build differs from the oracle (FP32
+accept / reject flips at triangle edges and caustic folds).  The FP64 error of every image
+is printed and bounded.  Scenes: single-refraction heightfield lens (T), two-sheet lens
+(TT), and 20,000 random pixels of the dispersive sphere frame (icosphere-5, 64 bins).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from palzilla_b200 import _lib
+from palzilla_b200 import api as A
+from palzilla_b200 import scenes as S
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    a = a.astype(np.float64)
+    b = b.astype(np.float64)
+    return float(np.sqrt(((a - b) ** 2).mean()) / max(np.sqrt((b ** 2).mean()), 1e-30))
+
+
+def _prepare(sc, iteration=0, capacity=1 << 22, path_capacity=1 << 23):
+    ds = A.DeviceScene(sc)
+    frame = A.Frame(sc, path_capacity=path_capacity)
+    A.solve_primary(ds, frame, iteration=iteration)
+    cache = A.PathCache(capacity=capacity, step=sc.cell_step)
+    A.photon_trace(ds, cache, iteration=iteration)
+    n = A.lookup_flatten(frame, cache, S.event_descriptor(sc.events))
+    A.sort_and_reorder(frame, n, A.OnesweepSort())
+    return ds, frame, cache, n
+
+
+def _solve(ds, frame, cache, sc, n, mode, scratch=None, stats=None, polish_det=0.0):
+    spectral = torch.zeros((sc.width * sc.height, sc.n_bins), device="cuda")
+    etas = torch.from_numpy(sc.bin_etas()).cuda()
+    d = A.solve_desc(ds, frame, cache, sc.events, n, spectral=spectral, etas=etas, stats=stats,
+                     exact=(mode == "exact"), polish_det=polish_det)
+    if mode == "batched":
+        A.solve_specular_batched(d, scratch if scratch is not None else A.Scratch())
+    else:
+        A.solve_specular_plain(d)
+    torch.cuda.synchronize()
+    return spectral.cpu().numpy()
+
+
+def _oracle_images(orc, sc, frame, cache, n, pixels=None):
+    pairs = frame.paths[: n * 8].cpu().numpy().view(np.int32).reshape(-1, 2).copy()
+    if pixels is not None:
+        pairs = pairs[np.isin(pairs[:, 0], pixels)].copy()
+    gc = cache.to_host()
+    fd = frame.fd.cpu().numpy().view(np.float32).reshape(-1, 10)
+    bvh = orc.build_bvh(sc.tris)
+    K = len(sc.events)
+    f32, _ = orc.render_pairs(K, pairs, gc, fd, bvh, sc, sc.bin_etas())
+    f64, _ = orc.render_pairs(K, pairs, gc, fd, bvh, sc, sc.bin_etas(), dtype=np.float64)
+    return f32, f64
+
+
+@pytest.mark.parametrize("events,side", [("T", 64), ("TT", 40)])
+def test_batched_lens_matches_plain_and_oracle(orc, events, side):
+    sc = S.lens_scene(side=side, seed=21, width=128, height=128, n_bins=16, events=events)
+    ds, frame, cache, n = _prepare(sc)
+    assert n > 1000
+    scratch = A.Scratch()
+    st_b = torch.zeros(3, dtype=torch.int64, device="cuda")
+    img_b = _solve(ds, frame, cache, sc, n, "batched", scratch, st_b)
+    img_p = _solve(ds, frame, cache, sc, n, "plain")
+    img_x = _solve(ds, frame, cache, sc, n, "exact")
+    f32, f64 = _oracle_images(orc, sc, frame, cache, n)
+    cnt = A.batched_counters(scratch)
+    assert cnt["skipped"] + cnt["predicted"] + cnt["fallback"] == n
+    assert int(st_b[0].item()) == n * sc.n_bins
+    assert scratch.status() == 0
+    r = {"batched_vs_plain_exact": _rel(img_b, img_x), "batched_vs_oracle": _rel(img_b, f32),
+         "plain_exact_vs_oracle": _rel(img_x, f32), "batched_vs_plain": _rel(img_b, img_p),
+         "plain_vs_oracle": _rel(img_p, f32), "batched_vs_fp64": _rel(img_b, f64), "oracle_vs_fp64": _rel(f32, f64)}
+    print(f"\n[{events}] n={n} " + " ".join(f"{k}={v:.2e}" for k, v in r.items()) + f" counters={cnt}")
+    assert r["plain_exact_vs_oracle"] <= 1e-5
+    assert r["batched_vs_oracle"] <= 1e-5
+    assert r["batched_vs_plain_exact"] <= 1e-5
+    assert r["batched_vs_plain"] <= max(1e-3, 1.5 * r["plain_vs_oracle"])
+    assert r["batched_vs_fp64"] <= max(1.01 * r["oracle_vs_fp64"], 1e-5)
+
+
+def test_batched_fp64_polish(orc):
+    """With polish_det = 1e-6, roots of near-singular Jacobians are refined in FP64 (and their
+    throughput evaluated in FP64); the image moves off the reference's float arithmetic by a
+    bounded amount and its FP64 error is reported."""
+    sc = S.lens_scene(side=40, seed=21, width=128, height=128, n_bins=16, events="TT")
+    ds, frame, cache, n = _prepare(sc)
+    scratch = A.Scratch()
+    img_b = _solve(ds, frame, cache, sc, n, "batched", scratch, polish_det=1e-6)
+    f32, f64 = _oracle_images(orc, sc, frame, cache, n)
+    cnt = A.batched_counters(scratch)
+    r = {"polished_vs_oracle": _rel(img_b, f32), "polished_vs_fp64": _rel(img_b, f64),
+         "oracle_vs_fp64": _rel(f32, f64)}
+    print("\n[TT polish] " + " ".join(f"{k}={v:.2e}" for k, v in r.items()) + f" polished={cnt['fp64_polish']}")
+    assert cnt["fp64_polish"] > 0
+    assert r["polished_vs_oracle"] <= 1e-3
+    assert r["polished_vs_fp64"] <= 2.0 * r["oracle_vs_fp64"]
+
+
+def test_batched_sphere_sample(orc):
+    """Dispersive sphere at full size; the oracle checks 20,000 random pixels (all their
+    work items x 64 bins)."""
+    sc = S.sphere_scene()
+    sc.photons_per_triangle = 205
+    ds, frame, cache, n = _prepare(sc, iteration=3, path_capacity=1 << 25)
+    img_b = _solve(ds, frame, cache, sc, n, "batched")
+    img_x = _solve(ds, frame, cache, sc, n, "exact")
+    img_p = _solve(ds, frame, cache, sc, n, "plain")
+    pairs = frame.paths[: n * 8].cpu().numpy().view(np.int32).reshape(-1, 2)
+    px = np.sort(np.random.default_rng(5).choice(np.unique(pairs[:, 0]), 20000, replace=False))
+    f32, f64 = _oracle_images(orc, sc, frame, cache, n, pixels=px)
+    r = {"batched_vs_oracle": _rel(img_b[px], f32[px]), "plain_exact_vs_oracle": _rel(img_x[px], f32[px]),
+         "batched_vs_fp64": _rel(img_b[px], f64[px]), "oracle_vs_fp64": _rel(f32[px], f64[px]),
+         "plain_vs_oracle": _rel(img_p[px], f32[px]), "full_batched_vs_plain_exact": _rel(img_b, img_x),
+         "full_batched_vs_plain": _rel(img_b, img_p), "full_plain_vs_plain_exact": _rel(img_p, img_x)}
+    print("\n[sphere] " + " ".join(f"{k}={v:.2e}" for k, v in r.items()))
+    assert r["plain_exact_vs_oracle"] <= 1e-5
+    assert r["batched_vs_oracle"] <= 1e-5
+    assert r["full_batched_vs_plain_exact"] <= 1e-5
+    assert r["batched_vs_fp64"] <= max(1.01 * r["oracle_vs_fp64"], 1e-5)
+    # the plain FMA build flips single (pixel, bin) entries at edges and folds
+    assert r["full_batched_vs_plain"] <= max(1e-3, 1.5 * r["full_plain_vs_plain_exact"])
+
+
+def test_batched_host_checks():
+    L = _lib.lib()
+    sc = S.lens_scene(side=16, seed=1, width=32, height=32, n_bins=4, events="T")
+    ds, frame, cache, n = _prepare(sc, capacity=1 << 20, path_capacity=1 << 18)
+    assert n > 16
+    spectral = torch.zeros((sc.width * sc.height, sc.n_bins), device="cuda")
+    etas = torch.from_numpy(sc.bin_etas()).cuda()
+    s = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    need = L.pz_solve_batched_scratch_bytes(1, n)
+    small = torch.empty(need - 256, dtype=torch.uint8, device="cuda")
+    d = A.solve_desc(ds, frame, cache, sc.events, n, spectral=spectral, etas=etas)
+    r = L.pz_solve_specular_batched(C.byref(d), None, C.c_void_p(small.data_ptr()), C.c_size_t(small.numel()), 0, s)
+    assert r == 2 and b"scratch" in L.pz_last_error()
+    d0 = A.solve_desc(ds, frame, cache, sc.events, 0, spectral=spectral, etas=etas)
+    r = L.pz_solve_specular_batched(C.byref(d0), None, C.c_void_p(small.data_ptr()), C.c_size_t(small.numel()), 0, s)
+    assert r == 0
+    dr = A.solve_desc(ds, frame, cache, sc.events, n)  # no spectral image: binned mode is required
+    big = torch.empty(need, dtype=torch.uint8, device="cuda")
+    r = L.pz_solve_specular_batched(C.byref(dr), None, C.c_void_p(big.data_ptr()), C.c_size_t(big.numel()), 0, s)
+    assert r == 1
+    torch.cuda.synchronize()
+    assert float(spectral.abs().sum()) == 0.0
+
+
+def test_batched_device_count():
+    """The item count read on the device (the lookup counter) gives the same image as the
+    host count."""
+    sc = S.lens_scene(side=32, seed=4, width=64, height=64, n_bins=8, events="T")
+    ds, frame, cache, n = _prepare(sc, path_capacity=1 << 20)
+    etas = torch.from_numpy(sc.bin_etas()).cuda()
+    imgs = []
+    for dev in (False, True):
+        spectral = torch.zeros((sc.width * sc.height, sc.n_bins), device="cuda")
+        d = A.solve_desc(ds, frame, cache, sc.events, frame.path_capacity if dev else n, spectral=spectral, etas=etas)
+        A.solve_specular_batched(d, A.Scratch(), n_paths_dev=frame.counter if dev else None)
+        torch.cuda.synchronize()
+        imgs.append(spectral.cpu().numpy())
+    assert _rel(imgs[1], imgs[0]) <= 1e-6
