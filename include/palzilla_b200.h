@@ -254,6 +254,32 @@ PZ_API size_t pz_solve_batched_scratch_bytes(int K, uint64_t max_paths);
 PZ_API int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32_t* n_paths_dev, void* scratch_dev,
                                      size_t scratch_bytes, int blocks_per_sm, pz_stream_t stream);
 
+/* ---------------------------------------------------------------- Path Cuts
+ * InternalNormalBound (pk.h:1705-1709, 52 B): for each internal node, the bounds of the
+ * shading normals of the triangles under each child. */
+typedef struct pz_normal_bound { pz_aabb normal_bounds[2]; uint32_t counter; } pz_normal_bound;
+/* Normal bounds of a BVH from pz_bvh_build (main.cpp:250-295), for its n_internals nodes. */
+PZ_API int pz_normal_bounds(const pz_internal_node* internals_dev, int n_internals,
+                            const pz_triangle_attrib* attribs_dev, pz_normal_bound* out_dev, pz_stream_t stream);
+/* Scratch for pz_path_cuts: a 256-byte header and two frontiers of frontier_capacity node
+ * tuples (at least n_queries; more lets wider trees through). */
+PZ_API size_t pz_path_cuts_scratch_bytes(int K, uint32_t frontier_capacity);
+/* Replaces traverseAdmissibleNodes<K> (pk.h:1760-2220) for a batch of queries: every
+ * admissible K-triangle tuple of the event chain `events` from p_beg to each p_end_dev[q],
+ * found by interval culling over BVH node tuples (BVH built with
+ * PZ_BUILD_OPTION_USE_NORMAL in the reference's use).  Writes (1 + K) u32 per tuple
+ * {q, triangle[0..K)} to tuples_dev (unordered), and the tuple count (which may exceed
+ * tuple_capacity: PZ_ERR_DEVICE is then returned) to *n_tuples_out, and the number of
+ * node tuples tested to *node_tuples_out (may be NULL).  directed_rounding = 0 runs the
+ * reference's round-to-nearest arithmetic (the same tuple set); 1 rounds every interval
+ * bound outward (a superset).  Synchronises `stream` once per tree level. */
+PZ_API int pz_path_cuts(int K, uint32_t events, float eta, pz_float3 p_beg, const pz_float3* p_end_dev,
+                        uint32_t n_queries, const pz_internal_node* internals_dev, const pz_normal_bound* nbs_dev,
+                        const pz_triangle* triangles_dev, const pz_triangle_attrib* attribs_dev,
+                        const uint32_t* root_dev, int directed_rounding, uint32_t* tuples_dev, uint32_t tuple_capacity,
+                        uint64_t* n_tuples_out, uint64_t* node_tuples_out, void* scratch_dev, size_t scratch_bytes,
+                        pz_stream_t stream);
+
 /* ---------------------------------------------------------------- resolve
  * pack (main_gpu.cu:499-513): accumulator / count -> sRGB OETF -> RGBA8. */
 PZ_API int pz_resolve(uint32_t* pixels_dev, const float* accum_dev, int n_pixels, pz_stream_t stream);

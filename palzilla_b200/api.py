@@ -324,3 +324,46 @@ def resolve_spectral(spectral, scene, rgb=None, pixels=None, stream=None):
     _lib.call("pz_resolve_spectral", _vp(rgb), _vp(pixels), _vp(spectral), C.c_int(scene.width * scene.height),
               C.c_int(scene.n_bins), C.c_float(scene.lambda_min), C.c_float(scene.lambda_max), _lib.f3(scene.albedo),
               C.c_void_p(_stream(stream)))
+
+
+# ---------------------------------------------------------------------------------------
+# Path Cuts
+# ---------------------------------------------------------------------------------------
+NORMAL_BOUND_BYTES = 52
+
+
+def normal_bounds(builder: BVHGPUBuilder, attribs, stream=None):
+    """InternalNormalBound array (pk.h:1705-1709) of a built BVH: uint8 tensor of
+    (n - 1) * 52 bytes."""
+    n = builder.m_nTriangles
+    out = torch.empty(max(n - 1, 1) * NORMAL_BOUND_BYTES, dtype=torch.uint8, device=attribs.device)
+    _lib.call("pz_normal_bounds", _vp(builder.m_internals), C.c_int(max(n - 1, 0)), _vp(attribs), _vp(out),
+              C.c_void_p(_stream(stream)))
+    return out
+
+
+class PathCuts:
+    """traverseAdmissibleNodes<K> (pk.h:1760-2220) for a batch of receiver points.
+
+    ``run(K, events, eta, p_beg, p_end, builder, nbs, triangles, attribs, directed)`` returns
+    an int32 tensor (n, 1 + K) of {query, triangle[K]} rows and the number of node tuples
+    tested."""
+
+    def __init__(self, device="cuda", frontier_capacity: int = 1 << 22, tuple_capacity: int = 1 << 22):
+        self.device = device
+        self.frontier_capacity = frontier_capacity
+        self.tuple_capacity = tuple_capacity
+        self.scratch = Scratch(device)
+
+    def run(self, K: int, events: int, eta: float, p_beg, p_end, builder: BVHGPUBuilder, nbs, triangles, attribs,
+            directed: bool = False, stream=None):
+        nq = p_end.shape[0]
+        cap = max(self.frontier_capacity, nq)
+        buf = self.scratch.get(_lib.lib().pz_path_cuts_scratch_bytes(K, cap))
+        out = torch.empty((self.tuple_capacity, 1 + K), dtype=torch.int32, device=self.device)
+        nt, visited = C.c_uint64(0), C.c_uint64(0)
+        _lib.call("pz_path_cuts", C.c_int(K), C.c_uint32(events), C.c_float(eta), _lib.f3(p_beg), _vp(p_end),
+                  C.c_uint32(nq), _vp(builder.m_internals), _vp(nbs), _vp(triangles), _vp(attribs),
+                  _vp(builder.m_rootNode), C.c_int(1 if directed else 0), _vp(out), C.c_uint32(self.tuple_capacity),
+                  C.byref(nt), C.byref(visited), _vp(buf), C.c_size_t(buf.numel()), C.c_void_p(_stream(stream)))
+        return out[: nt.value], visited.value

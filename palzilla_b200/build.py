@@ -37,6 +37,7 @@ UNITS = {
     "pz_capi": ("pz_capi.cu", []),
     "pz_capi_frame": ("pz_capi_frame.cu", []),
     "pz_sort_static": ("pz_sort_static.cu", []),
+    "pz_pathcuts": ("pz_pathcuts.cu", ["-fmad=false"]),
 }
 
 
