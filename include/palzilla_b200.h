@@ -280,6 +280,22 @@ PZ_API int pz_path_cuts(int K, uint32_t events, float eta, pz_float3 p_beg, cons
                         uint64_t* n_tuples_out, uint64_t* node_tuples_out, void* scratch_dev, size_t scratch_bytes,
                         pz_stream_t stream);
 
+/* ---------------------------------------------------------------- adjoint
+ * No reference counterpart.  A forward / backward pair for gradients of a loss on the
+ * binned spectral image.  Forward: the plain binned solve in the reference's arithmetic
+ * (exact_arithmetic is implied) into desc->spectral.  Backward (same descriptor and work
+ * list, geometry unchanged since the forward): recomputes each path's root from the
+ * photon's barycentrics, and for every accepted, unclamped path adds
+ * dL/dI[pixel][bin] * dI/dp to the gradients, by the implicit-function theorem at the
+ * root: grad_heights_dev[v] += dL/d(y of vertex v) through corner_vertex_dev (3 int32 per
+ * triangle: the vertex whose height is that corner's y, or -1), grad_cauchy_dev[0..1] +=
+ * dL/dA, dL/dB of eta = A + B / lambda^2.  The gradient arrays accumulate (clear them
+ * first).  K = 1 or 2. */
+PZ_API int pz_adjoint_forward(const pz_solve_desc* desc, pz_stream_t stream);
+PZ_API int pz_adjoint_backward(const pz_solve_desc* desc, const float* dloss_dspectral_dev,
+                               const int32_t* corner_vertex_dev, float* grad_heights_dev, float* grad_cauchy_dev,
+                               pz_stream_t stream);
+
 /* ---------------------------------------------------------------- resolve
  * pack (main_gpu.cu:499-513): accumulator / count -> sRGB OETF -> RGBA8. */
 PZ_API int pz_resolve(uint32_t* pixels_dev, const float* accum_dev, int n_pixels, pz_stream_t stream);

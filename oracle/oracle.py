@@ -270,6 +270,22 @@ class CpuLib:
         self.f("render_pairs", C.c_int)(*args)
         return spectral, stats
 
+    def render_each(self, K, pairs, cache, first_diffuse, bvh, scene, etas, max_iter=32, tol=1e-10, warmup=1,
+                    dtype=np.float64):
+        """Contribution of every (pair, bin) before the clamp (0 = rejected), (n_pairs, n_bins) float64."""
+        pairs = np.ascontiguousarray(pairs, np.int32)
+        etas = np.ascontiguousarray(etas, np.float32)
+        out = np.zeros((pairs.shape[0], etas.size), np.float64)
+        from palzilla_b200.scenes import event_descriptor
+        self.f("render_each", C.c_int)(
+            C.c_int(K), C.c_int(0 if dtype == np.float32 else 1), _p(pairs), C.c_int64(pairs.shape[0]),
+            _p(cache["tris"]), _p(cache["params"]), _p(np.ascontiguousarray(first_diffuse, np.float32)),
+            _p(bvh["nodes"]), C.c_uint32(bvh["root"]), _p(scene.tris), _p(scene.attribs),
+            _p(np.asarray(scene.p_light, np.float32)), C.c_float(scene.light_intensity),
+            C.c_uint32(event_descriptor(scene.events)), _p(etas), C.c_int(etas.size), C.c_int(max_iter),
+            C.c_float(tol), C.c_int(warmup), _p(out))
+        return out
+
     # ------------------------------------------------------------------ interval / path cuts
     def interval_square(self, l, u):
         out = np.zeros(2, np.float32)

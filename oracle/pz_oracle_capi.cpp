@@ -449,6 +449,43 @@ static void render_pairs(const int32_t* pairs, int64_t nPairs, const int32_t* sl
     stats[1] = conv;
     stats[2] = contrib;
 }
+// Per-path contributions (before the clamp; 0 = rejected) of every (pair, bin), for the
+// finite-difference references of the adjoint: the set of accepted paths can then be held
+// fixed across the perturbed renders.
+template <class T, int K>
+static void render_each(const int32_t* pairs, int64_t nPairs, const int32_t* slotTris, const float* slotParams,
+                        const float* firstDiffuse, const InternalNode* nodes, uint32_t root, const Triangle* tris,
+                        const TriangleAttrib* attribs, F3 L, float lightIntensity, uint32_t events, const float* etas,
+                        int nBins, int maxIter, float tol, int warmup, double* out)
+{
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t q = 0; q < nPairs; q++) {
+        int px = pairs[2 * q], slot = pairs[2 * q + 1];
+        const float* fd = firstDiffuse + 10 * (size_t)px;
+        V3<T> p = mk((T)fd[0], (T)fd[1], (T)fd[2]);
+        V3<T> n = mk((T)fd[3], (T)fd[4], (T)fd[5]);
+        Triangle tk[K];
+        TriangleAttrib ak[K];
+        for (int k = 0; k < K; k++) { tk[k] = tris[slotTris[4 * slot + k]]; ak[k] = attribs[slotTris[4 * slot + k]]; }
+        for (int b = 0; b < nBins; b++) {
+            double c = 0.0;
+            T prm[2 * K];
+            for (int i = 0; i < 2 * K; i++) prm[i] = (T)slotParams[8 * slot + i];
+            T eta = (T)etas[b];
+            V3<T> Lt = mk((T)L.x, (T)L.y, (T)L.z);
+            if (solve_constraints<T, K>(prm, Lt, p, tk, ak, eta, events, maxIter, (T)tol, warmup)) {
+                T thr = contributable_throughput<T, K>(prm, Lt, p, tk, ak, events, nodes, tris, root, eta);
+                if (T(0) < thr) {
+                    T dadw = dAdw<T>(Lt, get_vertex<T>(0, tk, prm) - Lt, p, tk, ak, events, eta);
+                    T cosv = std::fmax(dot(normalize(get_vertex<T>(K - 1, tk, prm) - p), n), T(0));
+                    c = (double)(thr * (T)lightIntensity / dadw * cosv);
+                }
+            }
+            out[(size_t)q * nBins + b] = c;
+        }
+    }
+}
+
 extern "C" {
 
 int pzo_render_pairs(int K, int dtype, const int32_t* pairs, int64_t nPairs, const int32_t* slotTris,
@@ -477,6 +514,31 @@ int pzo_render_pairs(int K, int dtype, const int32_t* pairs, int64_t nPairs, con
         default: return -1;
     }
 #undef PZO_R
+}
+
+int pzo_render_each(int K, int dtype, const int32_t* pairs, int64_t nPairs, const int32_t* slotTris,
+                    const float* slotParams, const float* firstDiffuse, const InternalNode* nodes, uint32_t root,
+                    const Triangle* tris, const TriangleAttrib* attribs, const float* p_light, float lightIntensity,
+                    uint32_t events, const float* etas, int nBins, int maxIter, float tol, int warmup, double* out)
+{
+    F3 L = ld3(p_light);
+#define PZO_E(KK)                                                                                                  \
+    case KK:                                                                                                       \
+        if (dtype == 0)                                                                                            \
+            render_each<float, KK>(pairs, nPairs, slotTris, slotParams, firstDiffuse, nodes, root, tris, attribs, L, \
+                                   lightIntensity, events, etas, nBins, maxIter, tol, warmup, out);                \
+        else                                                                                                       \
+            render_each<double, KK>(pairs, nPairs, slotTris, slotParams, firstDiffuse, nodes, root, tris, attribs,  \
+                                    L, lightIntensity, events, etas, nBins, maxIter, tol, warmup, out);            \
+        return 0;
+    switch (K) {
+        PZO_E(1)
+        PZO_E(2)
+        PZO_E(3)
+        PZO_E(4)
+        default: return -1;
+    }
+#undef PZO_E
 }
 
 // ---------------------------------------------------------------- interval + path cuts

@@ -78,6 +78,8 @@ SIGNATURES = {
     "pz_path_cuts_scratch_bytes": (sz, [i32, u32]),
     "pz_path_cuts": (i32, [i32, u32, f32, Float3, vp, u32, vp, vp, vp, vp, vp, i32, vp, u32, C.POINTER(u64),
                            C.POINTER(u64), vp, sz, vp]),
+    "pz_adjoint_forward": (i32, [C.POINTER(SolveDesc), vp]),
+    "pz_adjoint_backward": (i32, [C.POINTER(SolveDesc), vp, vp, vp, vp, vp]),
     "pz_resolve": (i32, [vp, vp, i32, vp]),
     "pz_resolve_spectral": (i32, [vp, vp, vp, i32, i32, f32, f32, Float3, vp]),
 }

@@ -38,6 +38,7 @@ UNITS = {
     "pz_capi_frame": ("pz_capi_frame.cu", []),
     "pz_sort_static": ("pz_sort_static.cu", []),
     "pz_pathcuts": ("pz_pathcuts.cu", ["-fmad=false"]),
+    "pz_adjoint": ("pz_adjoint.cu", ["-fmad=false"]),
 }
 
 

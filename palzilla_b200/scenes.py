@@ -137,6 +137,17 @@ def heightfield_lens(side: int = 64, seed: int = 1, amplitude: float = 0.01, n_t
     return tris.reshape(-1, 9).astype(np.float32), _attribs(norms, material)
 
 
+def heightfield_corners(side: int) -> np.ndarray:
+    """Grid vertex (row * side + column) of every corner of heightfield_lens' triangles,
+    (n_triangles, 3) int32 in the same order as its triangles."""
+    i, j = np.meshgrid(np.arange(side - 1), np.arange(side - 1), indexing="xy")
+    i, j = i.ravel(), j.ravel()
+    a, b, c, d = j * side + i, j * side + i + 1, (j + 1) * side + i + 1, (j + 1) * side + i
+    t0 = np.stack([a, d, b], 1)
+    t1 = np.stack([b, d, c], 1)
+    return np.stack([t0, t1], 1).reshape(-1, 3).astype(np.int32)
+
+
 def icosphere(subdivisions: int = 5, radius: float = 0.5, center=(0.0, 1.0, 0.0), material: int = MATERIAL_DIELECTRIC):
     """Icosphere with 20 * 4^subdivisions triangles, outward winding, smooth normals."""
     t = (1.0 + math.sqrt(5.0)) / 2.0
@@ -232,6 +243,22 @@ def lens_scene(side: int = 64, seed: int = 1, amplitude: float = 0.01, events: s
     cam = Camera(eye=(0.0, eye_y, 0.0), center=(0.0, 0.0, 0.0), up=(0.0, 0.0, -1.0), fovy=fovy)
     return Scene(name=name or f"lens{side}", tris=tris, attribs=att, camera=cam, events=events, n_bins=n_bins,
                  width=width, height=height)
+
+
+def adjoint_scene(side: int = 128, seed: int = 1, width: int = 512, height: int = 512, n_bins: int = 8,
+                  amplitude: float = 0.01):
+    """Heightfield lens for gradient checks: the lens_scene with a side x side grid (the
+    heightfield's triangles first) and the corner -> grid vertex map of every triangle
+    (-1 for the receiver).  Returns (scene, corners, initial heights per grid vertex)."""
+    sc = lens_scene(side=side, seed=seed, amplitude=amplitude, events="T", n_bins=n_bins, width=width, height=height,
+                    name=f"adjoint{side}")
+    hf = heightfield_corners(side)
+    corners = np.full((sc.n, 3), -1, np.int32)
+    corners[: hf.shape[0]] = hf
+    heights = np.zeros(side * side, np.float32)
+    ys = sc.tris[: hf.shape[0]].reshape(-1, 3, 3)[:, :, 1]
+    heights[hf.ravel()] = ys.ravel()
+    return sc, corners, heights
 
 
 def sphere_scene(subdivisions: int = 5, n_bins: int = 64, width: int = 1024, height: int = 1024) -> Scene:
