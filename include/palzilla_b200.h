@@ -254,6 +254,31 @@ PZ_API size_t pz_solve_batched_scratch_bytes(int K, uint64_t max_paths);
 PZ_API int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32_t* n_paths_dev, void* scratch_dev,
                                      size_t scratch_bytes, int blocks_per_sm, pz_stream_t stream);
 
+/* ---------------------------------------------------------------- batches of scenes
+ * No reference counterpart.  Many scenes (each with its own triangles, BVH, PathCache,
+ * eye pass, work list and spectral image; one K and one bin count for all) solved by the
+ * batched persistent solver in one set of launches: one device work queue over the
+ * concatenated work items of every scene, each item solving in its own scene.
+ * pz_solve_multi_prepare uploads the scene table into the scratch (synchronises the
+ * stream: do it before any stream capture); n_paths_dev[i] is scene i's device item count
+ * (e.g. its lookup counter; NULL entries or a NULL array: descs[i].n_paths), descs[i].n_paths
+ * its capacity.  pz_solve_specular_multi then only enqueues work (memsets and kernels), so
+ * a frame that calls it can be captured in a CUDA graph.  Tuning: probe / phase-1 blocks per
+ * SM, phase-2 blocks per SM (1 or 2) and records per phase-2 queue access; NULL = the best
+ * found by pz_solve_multi_autotune for this (K, bins, capacity), else {8, 2, 1}.
+ * pz_solve_multi_autotune renders the batch once per candidate (clear the images after
+ * it) and keeps the fastest. */
+typedef struct pz_batch_tuning { int p1_blocks_per_sm, p2_blocks_per_sm, p2_chunk; } pz_batch_tuning;
+PZ_API size_t pz_solve_multi_scratch_bytes(int K, uint32_t n_scenes, uint64_t max_paths_total);
+PZ_API int pz_solve_multi_prepare(const pz_solve_desc* descs, const uint32_t* const* n_paths_dev, uint32_t n_scenes,
+                                  void* scratch_dev, size_t scratch_bytes, pz_stream_t stream);
+PZ_API int pz_solve_specular_multi(int K, int n_bins, uint32_t n_scenes, uint64_t max_paths_total, void* scratch_dev,
+                                   size_t scratch_bytes, const pz_batch_tuning* tuning, unsigned long long* stats_dev,
+                                   pz_stream_t stream);
+PZ_API int pz_solve_multi_autotune(int K, int n_bins, uint32_t n_scenes, uint64_t max_paths_total, void* scratch_dev,
+                                   size_t scratch_bytes, unsigned long long* stats_dev, pz_batch_tuning* best_out,
+                                   float* best_ms_out, pz_stream_t stream);
+
 /* ---------------------------------------------------------------- Path Cuts
  * InternalNormalBound (pk.h:1705-1709, 52 B): for each internal node, the bounds of the
  * shading normals of the triangles under each child. */

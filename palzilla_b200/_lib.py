@@ -34,6 +34,10 @@ class LensParams(C.Structure):
     _fields_ = [("distance", f32), ("thickness", f32), ("R", f32)]
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("p1_blocks_per_sm", C.c_int), ("p2_blocks_per_sm", C.c_int), ("p2_chunk", C.c_int)]
+
+
 class SolveDesc(C.Structure):
     _fields_ = [("K", i32), ("events", u32), ("paths", vp), ("n_paths", u64), ("first_diffuse", vp),
                 ("internals", vp), ("root", vp), ("triangles", vp), ("attribs", vp), ("cache", vp),
@@ -74,6 +78,10 @@ SIGNATURES = {
     "pz_solve_specular_plain": (i32, [C.POINTER(SolveDesc), vp]),
     "pz_solve_batched_scratch_bytes": (sz, [i32, u64]),
     "pz_solve_specular_batched": (i32, [C.POINTER(SolveDesc), vp, vp, sz, i32, vp]),
+    "pz_solve_multi_scratch_bytes": (sz, [i32, u32, u64]),
+    "pz_solve_multi_prepare": (i32, [vp, vp, u32, vp, sz, vp]),
+    "pz_solve_specular_multi": (i32, [i32, i32, u32, u64, vp, sz, vp, vp, vp]),
+    "pz_solve_multi_autotune": (i32, [i32, i32, u32, u64, vp, sz, vp, vp, vp, vp]),
     "pz_normal_bounds": (i32, [vp, i32, vp, vp, vp]),
     "pz_path_cuts_scratch_bytes": (sz, [i32, u32]),
     "pz_path_cuts": (i32, [i32, u32, f32, Float3, vp, u32, vp, vp, vp, vp, vp, i32, vp, u32, C.POINTER(u64),

@@ -367,3 +367,45 @@ class PathCuts:
                   _vp(builder.m_rootNode), C.c_int(1 if directed else 0), _vp(out), C.c_uint32(self.tuple_capacity),
                   C.byref(nt), C.byref(visited), _vp(buf), C.c_size_t(buf.numel()), C.c_void_p(_stream(stream)))
         return out[: nt.value], visited.value
+
+
+# ---------------------------------------------------------------------------------------
+# batches of scenes
+# ---------------------------------------------------------------------------------------
+class SceneBatch:
+    """Scenes of one K and bin count solved together by the batched persistent solver
+    (pz_solve_multi_prepare / pz_solve_specular_multi / pz_solve_multi_autotune).
+
+    ``descs``: one solve descriptor per scene (binned mode; n_paths = its capacity when
+    ``counts`` gives the device item counters, else its item count)."""
+
+    def __init__(self, descs, counts=None, device="cuda", stream=None):
+        n = len(descs)
+        self.K, self.n_bins, self.n = descs[0].K, descs[0].n_bins, n
+        self.total = sum(int(d.n_paths) for d in descs)
+        self._descs = (_lib.SolveDesc * n)(*descs)
+        self._counts = (C.c_void_p * n)(*[None if c is None else c.data_ptr() for c in (counts or [None] * n)])
+        nbytes = _lib.lib().pz_solve_multi_scratch_bytes(self.K, n, self.total)
+        self.scratch = torch.empty(nbytes, dtype=torch.uint8, device=device)
+        _lib.call("pz_solve_multi_prepare", C.cast(self._descs, C.c_void_p), C.cast(self._counts, C.c_void_p),
+                  C.c_uint32(n), _vp(self.scratch),
+                  C.c_size_t(nbytes), C.c_void_p(_stream(stream)))
+
+    def solve(self, tuning=None, stats=None, stream=None):
+        t = None if tuning is None else C.byref(_lib.BatchTuning(*tuning))
+        _lib.call("pz_solve_specular_multi", C.c_int(self.K), C.c_int(self.n_bins), C.c_uint32(self.n),
+                  C.c_uint64(self.total), _vp(self.scratch), C.c_size_t(self.scratch.numel()), t, _vp(stats),
+                  C.c_void_p(_stream(stream)))
+
+    def autotune(self, stats=None, stream=None):
+        """Renders the batch once per candidate (clear the images afterwards); returns the
+        fastest (p1_blocks_per_sm, p2_blocks_per_sm, p2_chunk) and its time in ms."""
+        best, ms = _lib.BatchTuning(), C.c_float(0.0)
+        _lib.call("pz_solve_multi_autotune", C.c_int(self.K), C.c_int(self.n_bins), C.c_uint32(self.n),
+                  C.c_uint64(self.total), _vp(self.scratch), C.c_size_t(self.scratch.numel()), _vp(stats),
+                  C.byref(best), C.byref(ms), C.c_void_p(_stream(stream)))
+        return (best.p1_blocks_per_sm, best.p2_blocks_per_sm, best.p2_chunk), ms.value
+
+    def counters(self) -> dict:
+        v = self.scratch[64:64 + 8 * len(BATCH_COUNTERS)].view(torch.int64).cpu().tolist()
+        return dict(zip(BATCH_COUNTERS, v))

@@ -1,10 +1,11 @@
-"""Builds the sm_100a CUDA library in-tree: palzilla_b200/libpalzilla_b200.so.
+"""Builds the sm_100a CUDA library in-tree: palzilla_b200/libpalzilla_b200.so, and the
+C++ facade's driver program palzilla_b200/pk_render.
 
 Each translation unit is compiled with nvcc for sm_100a.  Units whose results must
-be bit-exact with the CPU oracle (BVH keys, traversal, photons, eye pass) are built
-with -fmad=false so that no multiply-add pair is contracted into an FMA; the solver
-units keep FMA contraction.  Objects are rebuilt only when a source or header is
-newer than the object.
+be bit-exact with the CPU oracle (BVH keys, traversal, photons, eye pass, the batched
+solver, path cuts, the adjoint) are built with -fmad=false so that no multiply-add pair
+is contracted into an FMA; the plain solver is built both ways.  Objects are rebuilt
+only when a source or header is newer than the object.
 """
 from __future__ import annotations
 
@@ -18,6 +19,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libpalzilla_b200.so")
+PK_RENDER = os.path.join(HERE, "pk_render")
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -78,7 +81,22 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
+    build_pk_render(verbose)
     return LIB
+
+
+def build_pk_render(verbose: bool = False) -> str:
+    """The C++ facade's driver (include/palzilla_b200.hpp, cpp/pk_render.cpp)."""
+    src = os.path.join(HERE, "cpp", "pk_render.cpp")
+    hdrs = glob.glob(os.path.join(ROOT, "include", "*.h*"))
+    if _newer(PK_RENDER, [src, LIB] + hdrs):
+        cmd = ["g++", "-std=c++17", "-O2", "-I" + os.path.join(ROOT, "include"), "-I" + os.path.join(CUDA_HOME, "include"),
+               src, "-o", PK_RENDER, "-L" + HERE, "-lpalzilla_b200", "-L" + os.path.join(CUDA_HOME, "lib64"),
+               "-lcudart", "-Wl,-rpath,$ORIGIN", "-Wl,-rpath," + os.path.join(CUDA_HOME, "lib64")]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return PK_RENDER
 
 
 if __name__ == "__main__":

@@ -52,6 +52,7 @@ constexpr float kProbeTol = 1.0e-3f;  // a plain-solve root farther than this fr
 template <int K> struct PairRec {
     int pixel, slot, mode;  // mode 1: predicted roots, 2: plain per-bin solves
     int polish;             // the item is ill-conditioned: FP64 polish of its roots
+    int scene, pad;         // the item's scene in a batch of scenes
     unsigned long long mask;  // bins to solve (mode 1)
     unsigned long long warm;  // of those, bins whose root is deep inside: refine the prediction
     float xa[2 * K], xc[2 * K], xb[2 * K];  // roots at the first, centre and last bin
@@ -252,6 +253,63 @@ __device__ __noinline__ bool plain_solve(float* x, const Chain<K>& ch, float3 p_
                             &it, &det, 0);
 }
 
+// ---------------------------------------------------------------- scenes of a batch
+// A work item's scene: the single scene of the call, or, for a batch of scenes, the one
+// whose range of the concatenated item list holds it (offsets[s] <= idx < offsets[s + 1]).
+struct SceneRef {
+    const SolveArgs* s;
+    uint64_t local;
+    uint32_t scene;
+};
+PZ_D SceneRef item_scene(const BatchArgs& a, uint64_t idx)
+{
+    if (!a.scenes) return SceneRef{&a.s, idx, 0u};
+    uint32_t lo = 0, hi = a.nScenes;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (a.offsets[mid] <= idx) lo = mid;
+        else hi = mid;
+    }
+    return SceneRef{&a.scenes[lo].s, idx - a.offsets[lo], lo};
+}
+PZ_D uint64_t total_items(const BatchArgs& a)
+{
+    if (a.scenes) return a.offsets[a.nScenes];
+    return a.nPathsDev ? min((uint64_t)*a.nPathsDev, a.s.nPaths) : a.s.nPaths;
+}
+
+// Item offsets of a batch of scenes: exclusive scan of each scene's item count (its
+// device counter, capped at its capacity).  One block.
+__global__ void k_scene_offsets(const SceneArgs* scenes, uint32_t n, unsigned long long* offsets)
+{
+    __shared__ unsigned long long carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < n; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        unsigned long long c = 0;
+        if (i < n) {
+            const SceneArgs& sa = scenes[i];
+            c = sa.nPathsDev ? min((uint64_t)*sa.nPathsDev, sa.s.nPaths) : sa.s.nPaths;
+        }
+        // block-wide inclusive scan (Hillis-Steele in shared memory)
+        __shared__ unsigned long long buf[1024];
+        buf[threadIdx.x] = c;
+        __syncthreads();
+        for (uint32_t o = 1; o < blockDim.x; o <<= 1) {
+            const unsigned long long v = threadIdx.x >= o ? buf[threadIdx.x - o] : 0ull;
+            __syncthreads();
+            buf[threadIdx.x] += v;
+            __syncthreads();
+        }
+        if (i < n) offsets[i] = carry + buf[threadIdx.x] - c;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry += buf[threadIdx.x];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) offsets[n] = carry;
+}
+
 // ---------------------------------------------------------------- probes
 // One thread per (work item, probe bin): the plain path's solver from the photon's start at
 // the centre, first and last bin.  Kept apart from phase 1 so that it runs at the plain
@@ -260,19 +318,21 @@ template <int K>
 __global__ void __launch_bounds__(256) k_probe(BatchArgs a)
 {
     const int B = a.s.nBins;
-    const uint64_t nPaths = a.nPathsDev ? min((uint64_t)*a.nPathsDev, a.s.nPaths) : a.s.nPaths;
+    const uint64_t nPaths = total_items(a);
     auto* probes = reinterpret_cast<Probe<K>*>(a.probes);
-    const V3<float> L = v3f<float>(a.s.p_light);
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < 3 * nPaths;
          t += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t idx = t / 3;
         const int q = (int)(t - 3 * idx);
-        const SpecularPath sp = a.s.paths[idx];
-        const int4 ti = a.s.cache.tris[sp.cacheIndex];
+        const SceneRef R = item_scene(a, idx);
+        const SolveArgs& S = *R.s;
+        const V3<float> L = v3f<float>(S.p_light);
+        const SpecularPath sp = S.paths[R.local];
+        const int4 ti = S.cache.tris[sp.cacheIndex];
         const int tix[4] = {ti.x, ti.y, ti.z, ti.w};
         Chain<K> ch;
-        load_chain<K>(ch, a.s.tris, a.s.attribs, tix);
-        const float4 q0 = a.s.cache.params[2 * sp.cacheIndex], q1 = a.s.cache.params[2 * sp.cacheIndex + 1];
+        load_chain<K>(ch, S.tris, S.attribs, tix);
+        const float4 q0 = S.cache.params[2 * sp.cacheIndex], q1 = S.cache.params[2 * sp.cacheIndex + 1];
         const float pp[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
         Probe<K> r;
 #pragma unroll
@@ -280,8 +340,8 @@ __global__ void __launch_bounds__(256) k_probe(BatchArgs a)
         const int b = q == 0 ? B / 2 : (q == 1 ? 0 : B - 1);
         int it;
         float det;
-        r.ok = newton<float, K>(r.x, L, v3f<float>(a.s.fds[sp.pixel].p), ch, a.s.etas[b], a.s.events,
-                                a.s.maxIterations, a.s.costTolerance, a.s.earlyTermWarmUp, true, &it, &det, 0)
+        r.ok = newton<float, K>(r.x, L, v3f<float>(S.fds[sp.pixel].p), ch, S.etas[b], S.events, S.maxIterations,
+                                S.costTolerance, S.earlyTermWarmUp, true, &it, &det, 0)
                    ? 1u
                    : 0u;
         probes[t] = r;
@@ -293,25 +353,27 @@ template <int K>
 __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
 {
     const int B = a.s.nBins;
-    const uint64_t nPaths = a.nPathsDev ? min((uint64_t)*a.nPathsDev, a.s.nPaths) : a.s.nPaths;
+    const uint64_t nPaths = total_items(a);
     const int bc = B / 2;
-    const float eta_c = a.s.etas[bc];
-    const V3<float> L = v3f<float>(a.s.p_light);
     auto* recs = reinterpret_cast<PairRec<K>*>(a.records);
     unsigned long long nItems = 0;
     for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < nPaths;
          idx += (uint64_t)gridDim.x * blockDim.x) {
-        const SpecularPath sp = a.s.paths[idx];
-        const int4 ti = a.s.cache.tris[sp.cacheIndex];
+        const SceneRef R = item_scene(a, idx);
+        const SolveArgs& S = *R.s;
+        const float eta_c = S.etas[bc];
+        const V3<float> L = v3f<float>(S.p_light);
+        const SpecularPath sp = S.paths[R.local];
+        const int4 ti = S.cache.tris[sp.cacheIndex];
         const int tix[4] = {ti.x, ti.y, ti.z, ti.w};
         Chain<K> ch;
-        load_chain<K>(ch, a.s.tris, a.s.attribs, tix);
-        const float4 q0 = a.s.cache.params[2 * sp.cacheIndex], q1 = a.s.cache.params[2 * sp.cacheIndex + 1];
+        load_chain<K>(ch, S.tris, S.attribs, tix);
+        const float4 q0 = S.cache.params[2 * sp.cacheIndex], q1 = S.cache.params[2 * sp.cacheIndex + 1];
         const float pp[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
         float x[2 * K], xpc[2 * K];
 #pragma unroll
         for (int i = 0; i < 2 * K; i++) x[i] = xpc[i] = pp[i];
-        const V3<float> p = v3f<float>(a.s.fds[sp.pixel].p);
+        const V3<float> p = v3f<float>(S.fds[sp.pixel].p);
         int it;
         float det = 1.0f;
         // the plain path's decision at the centre bin (k_probe); when it converged, its root
@@ -325,11 +387,12 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
 #pragma unroll
             for (int i = 0; i < 2 * K; i++) x[i] = xpc[i];
         } else {
-            conv = newton<float, K>(x, L, p, ch, eta_c, a.s.events, 24, a.s.costTolerance, 0, false, &it, &det);
+            conv = newton<float, K>(x, L, p, ch, eta_c, S.events, 24, S.costTolerance, 0, false, &it, &det);
         }
         PairRec<K> r;
         r.pixel = sp.pixel;
         r.slot = sp.cacheIndex;
+        r.scene = (int)R.scene;
         r.mode = 2;
         r.polish = 0;
         r.mask = 0;
@@ -339,7 +402,7 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
             // root derivative in eta at the centre (implicit-function theorem) and the two
             // end-bin roots, warm-started from the tangent prediction
             float J[2 * K + 1][3 * K], c[3 * K], cost;
-            eval_constraints<float, K, true>(x, L, p, ch, eta_c, a.s.events, J, c, cost);
+            eval_constraints<float, K, true>(x, L, p, ch, eta_c, S.events, J, c, cost);
             float Jx[2 * K][3 * K], rhs[3 * K], dxe[2 * K];
 #pragma unroll
             for (int i = 0; i < 2 * K; i++)
@@ -348,7 +411,7 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
 #pragma unroll
             for (int j = 0; j < 3 * K; j++) rhs[j] = J[2 * K][j];
             det = qr_solve_reldet<float, 3 * K, 2 * K>(Jx, rhs, dxe);
-            const float ea = a.s.etas[0], eb = a.s.etas[B - 1];
+            const float ea = S.etas[0], eb = S.etas[B - 1];
             float lin_a[2 * K], lin_b[2 * K];
 #pragma unroll
             for (int i = 0; i < 2 * K; i++) {
@@ -361,9 +424,9 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
             int ia, ib;
             float da, db;
             const bool ca =
-                newton<float, K>(r.xa, L, p, ch, ea, a.s.events, 12, a.s.costTolerance, 0, false, &ia, &da, 1);
+                newton<float, K>(r.xa, L, p, ch, ea, S.events, 12, S.costTolerance, 0, false, &ia, &da, 1);
             const bool cb =
-                newton<float, K>(r.xb, L, p, ch, eb, a.s.events, 12, a.s.costTolerance, 0, false, &ib, &db, 1);
+                newton<float, K>(r.xb, L, p, ch, eb, S.events, 12, S.costTolerance, 0, false, &ib, &db, 1);
             float nonlin = 0.0f;
             bool finite = true;
 #pragma unroll
@@ -383,7 +446,7 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
                 unsigned long long mask = 0, warm = 0;
                 for (int b = 0; b < B; b++) {
                     float xp[2 * K];
-                    predict_root<K>(xp, r, a.s.etas[b], ea, eta_c, eb);
+                    predict_root<K>(xp, r, S.etas[b], ea, eta_c, eb);
                     float depth = 1.0f;
 #pragma unroll
                     for (int k = 0; k < K; k++)
@@ -466,25 +529,31 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
     const int B = a.s.nBins;
     const unsigned long long nRec = min(*a.recordCount, a.recordCapacity);
     const auto* recs = reinterpret_cast<const PairRec<K>*>(a.records);
-    const uint32_t root = __ldg(a.s.root);
-    const float eta_c = a.s.etas[B / 2];
-    const V3<float> L = v3f<float>(a.s.p_light);
+    const int chunk = a.chunk > 0 ? a.chunk : 1;
     unsigned long long nConv = 0, nContrib = 0;
+    unsigned long long j = 0, jEnd = 0;
     for (;;) {
-        unsigned long long j = 0;
-        if (lane == 0) j = atomicAdd(a.workCounter, 1ull);
-        j = __shfl_sync(0xFFFFFFFFu, j, 0);
+        // the warp takes `chunk` records at a time from the work counter
+        if (j >= jEnd) {
+            if (lane == 0) j = atomicAdd(a.workCounter, (unsigned long long)chunk);
+            j = __shfl_sync(0xFFFFFFFFu, j, 0);
+            jEnd = min(j + (unsigned long long)chunk, nRec);
+        }
         if (j >= nRec) break;
-        const PairRec<K> r = recs[j];
-        const int4 ti = a.s.cache.tris[r.slot];
+        const PairRec<K> r = recs[j++];
+        const SolveArgs& S = a.scenes ? a.scenes[r.scene].s : a.s;
+        const uint32_t root = __ldg(S.root);
+        const float eta_c = S.etas[B / 2];
+        const V3<float> L = v3f<float>(S.p_light);
+        const int4 ti = S.cache.tris[r.slot];
         const int tix[4] = {ti.x, ti.y, ti.z, ti.w};
         Chain<K> ch;
-        load_chain<K>(ch, a.s.tris, a.s.attribs, tix);
-        const FirstDiffuse fd = a.s.fds[r.pixel];
+        load_chain<K>(ch, S.tris, S.attribs, tix);
+        const FirstDiffuse fd = S.fds[r.pixel];
         const V3<float> p = v3f<float>(fd.p);
         float x0[2 * K];
         {
-            const float4 q0 = a.s.cache.params[2 * r.slot], q1 = a.s.cache.params[2 * r.slot + 1];
+            const float4 q0 = S.cache.params[2 * r.slot], q1 = S.cache.params[2 * r.slot + 1];
             const float pp[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
 #pragma unroll
             for (int i = 0; i < 2 * K; i++) x0[i] = pp[i];
@@ -504,10 +573,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
             float xs[2 * K];
             float thr = 0.0f;
             if (b < B) {
-                const float eta = a.s.etas[b];
+                const float eta = S.etas[b];
                 const bool warm = r.mode == 1 && (a.continuation || ((r.warm >> b) & 1ull));
                 if (warm) {
-                    predict_root<K>(xs, r, eta, a.s.etas[0], eta_c, a.s.etas[B - 1]);
+                    predict_root<K>(xs, r, eta, S.etas[0], eta_c, S.etas[B - 1]);
                 } else {
 #pragma unroll
                     for (int i = 0; i < 2 * K; i++) xs[i] = x0[i];
@@ -516,10 +585,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
                 float det = 1.0f;
                 // a predicted root is refined by Newton; every other bin runs the plain path's
                 // solver from the photon's start, so its accept / reject decision is the plain one
-                const bool conv = warm ? newton<float, K>(xs, L, p, ch, eta, a.s.events, a.s.maxIterations,
-                                                          a.s.costTolerance, a.s.earlyTermWarmUp, true, &it, &det, 1)
-                                       : plain_solve<K>(xs, ch, a.s.p_light, fd.p, eta, a.s.events, a.s.maxIterations,
-                                                        a.s.costTolerance, a.s.earlyTermWarmUp);
+                const bool conv = warm ? newton<float, K>(xs, L, p, ch, eta, S.events, S.maxIterations,
+                                                          S.costTolerance, S.earlyTermWarmUp, true, &it, &det, 1)
+                                       : plain_solve<K>(xs, ch, S.p_light, fd.p, eta, S.events, S.maxIterations,
+                                                        S.costTolerance, S.earlyTermWarmUp);
                 if (a.counters) atomicAdd(a.counters + kCntNewton2, 1ull);
                 if (conv) {
                     nConv++;
@@ -527,9 +596,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
                     if (polish && a.counters) atomicAdd(a.counters + kCntPolish, 1ull);
                     float3 vtx[K + 2], nrm[K + 2];
                     if (polish)
-                        thr = polish_fp64<K>(xs, ch, a.s.p_light, fd.p, a.s.events, eta, vtx, nrm);
+                        thr = polish_fp64<K>(xs, ch, S.p_light, fd.p, S.events, eta, vtx, nrm);
                     else
-                        thr = pre_throughput<float, K>(xs, L, p, ch, a.s.events, eta, vtx, nrm);
+                        thr = pre_throughput<float, K>(xs, L, p, ch, S.events, eta, vtx, nrm);
                 }
             }
             // shared visibility: one fattened query per segment for all bins of the round
@@ -540,8 +609,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
                 float3 sa = mk3(0.f, 0.f, 0.f), sb = mk3(0.f, 0.f, 0.f);
                 if (thr > 0.0f) {
                     float3 v0, n0, v1, n1;
-                    chain_vertex<K>(ch, xs, a.s.p_light, fd.p, s, v0, n0);
-                    chain_vertex<K>(ch, xs, a.s.p_light, fd.p, s + 1, v1, n1);
+                    chain_vertex<K>(ch, xs, S.p_light, fd.p, s, v0, n0);
+                    chain_vertex<K>(ch, xs, S.p_light, fd.p, s + 1, v1, n1);
                     shadow_segment(v0, n0, v1, n1, sa, sb);
                 }
                 const float3 ra = mk3(__shfl_sync(0xFFFFFFFFu, sa.x, leader), __shfl_sync(0xFFFFFFFFu, sa.y, leader),
@@ -558,7 +627,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
                 rad = warp_max(rad);
                 mag = warp_max(mag);
                 rad += 1.0e-5f * (1.0f + mag);  // covers the rounding of the slab and box arithmetic
-                const int nc = fat_query(a.s.nodes, a.s.tris, root, ra, rb, rad, cand[warp]);
+                const int nc = fat_query(S.nodes, S.tris, root, ra, rb, rad, cand[warp]);
                 __syncwarp();
                 if (lane == 0 && a.counters) {
                     atomicAdd(a.counters + kCntQueries, 1ull);
@@ -569,11 +638,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
                     const float3 d = ex::sub3(sb, sa);
                     bool occ = false;
                     if (nc < 0) {
-                        occ = any_hit(a.s.nodes, a.s.tris, root, sa, d, 1.0f) < 1.0f;
+                        occ = any_hit(S.nodes, S.tris, root, sa, d, 1.0f) < 1.0f;
                     } else {
                         for (int c = 0; c < nc && !occ; c++) {
                             float3 v0, v1, v2;
-                            load_tri(a.s.tris, cand[warp][c], v0, v1, v2);
+                            load_tri(S.tris, cand[warp][c], v0, v1, v2);
                             float t, u, v;
                             float3 ng;
                             if (ray_triangle(&t, &u, &v, &ng, 0.0f, 1.0f, sa, d, v0, v1, v2) && t < 1.0f) occ = true;
@@ -585,13 +654,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
             }
             if (thr > 0.0f) {
                 nContrib++;
-                const float eta = a.s.etas[b];
-                const float dadwv = dadw_out_of_line<K>(ch, xs, a.s.p_light, fd.p, a.s.events, eta);
+                const float eta = S.etas[b];
+                const float dadwv = dadw_out_of_line<K>(ch, xs, S.p_light, fd.p, S.events, eta);
                 const V3<float> vl = vertex<float, K>(ch, xs, K - 1);
                 const float cosv = fmaxf(vdot(vnormalize(vl - p), v3f<float>(fd.ng)), 0.0f);
-                float contrib = thr * a.s.lightIntensity / dadwv * cosv;
-                contrib = fminf(contrib, a.s.radianceClamp);
-                atomicAdd(a.s.spectral + (size_t)r.pixel * B + b, contrib);
+                float contrib = thr * S.lightIntensity / dadwv * cosv;
+                contrib = fminf(contrib, S.radianceClamp);
+                atomicAdd(S.spectral + (size_t)r.pixel * B + b, contrib);
             }
         }
     }
@@ -608,10 +677,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
 }
 
 template <int K>
-static cudaError_t launch_k(const BatchArgs& a, int blocksPerSM, cudaStream_t s)
+static cudaError_t launch_k(const BatchArgs& a, int blocksPerSM, cudaStream_t s, int p1BlocksPerSM = 8)
 {
-    k_probe<K><<<kNumSMs * 16, 256, 0, s>>>(a);
-    k_phase1<K><<<kNumSMs * 8, 256, 0, s>>>(a);
+    k_probe<K><<<kNumSMs * 2 * p1BlocksPerSM, 256, 0, s>>>(a);
+    k_phase1<K><<<kNumSMs * p1BlocksPerSM, 256, 0, s>>>(a);
     k_phase2<K><<<kNumSMs * blocksPerSM, kWarpsPerBlock * 32, 0, s>>>(a);
     return cudaGetLastError();
 }
@@ -649,6 +718,24 @@ cudaError_t launch_solve_batched(int K, const BatchArgs& a, int blocksPerSM, cud
         case 2: return launch_k<2>(a, blocksPerSM, s);
         case 3: return launch_k<3>(a, blocksPerSM, s);
         case 4: return launch_k<4>(a, blocksPerSM, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_solve_batched_multi(int K, const BatchArgs& a, int p1BlocksPerSM, int p2BlocksPerSM,
+                                       unsigned long long* offsets, cudaStream_t s)
+{
+    if (a.s.nBins < 1 || a.s.nBins > 64 || !a.scenes || a.nScenes == 0) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(a.workCounter, 0, sizeof(unsigned long long), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(a.recordCount, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
+    k_scene_offsets<<<1, 1024, 0, s>>>(a.scenes, a.nScenes, offsets);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    switch (K) {
+        case 1: return launch_k<1>(a, p2BlocksPerSM, s, p1BlocksPerSM);
+        case 2: return launch_k<2>(a, p2BlocksPerSM, s, p1BlocksPerSM);
+        case 3: return launch_k<3>(a, p2BlocksPerSM, s, p1BlocksPerSM);
+        case 4: return launch_k<4>(a, p2BlocksPerSM, s, p1BlocksPerSM);
     }
     return cudaErrorInvalidValue;
 }

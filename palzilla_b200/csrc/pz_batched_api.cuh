@@ -5,6 +5,8 @@
 namespace pz {
 namespace batched {
 
+struct SceneArgs;
+
 struct BatchArgs {
     SolveArgs s;                       // binned mode only (s.spectral, s.etas, s.nBins <= 64)
     const uint32_t* nPathsDev;         // device item count (the lookup counter), or null: s.nPaths
@@ -18,6 +20,16 @@ struct BatchArgs {
     double polishDet;                  // FP64 polish below this relative det (<= 0: never)
     int continuation;                  // 1: refine predicted roots instead of solving from the photon start
     float illDet;                      // relative det below which an item takes per-bin solves (near a fold)
+    int chunk = 0;                     // records a phase-2 warp takes per queue access (0: 1)
+    const SceneArgs* scenes = nullptr; // batch of scenes (device table), or null: the single scene s
+    uint32_t nScenes = 0;
+    const unsigned long long* offsets = nullptr;  // nScenes + 1 item offsets of the batch
+};
+
+// One scene of a batch: its solve arguments and its item count on the device.
+struct SceneArgs {
+    SolveArgs s;
+    const uint32_t* nPathsDev;         // or null: s.nPaths
 };
 
 // diagnostics counters
@@ -31,6 +43,10 @@ size_t record_bytes(int K);
 // bytes of one plain-solve probe (root and verdict) for chain length K
 size_t probe_bytes(int K);
 cudaError_t launch_solve_batched(int K, const BatchArgs& a, int blocksPerSM, cudaStream_t s);
+// Batch of scenes: item offsets (one small kernel) then the same three launches; the
+// tuning picks the probe / phase-1 grid (blocks per SM) and phase 2's blocks per SM.
+cudaError_t launch_solve_batched_multi(int K, const BatchArgs& a, int p1BlocksPerSM, int p2BlocksPerSM,
+                                       unsigned long long* offsets, cudaStream_t s);
 
 }  // namespace batched
 }  // namespace pz

@@ -1,6 +1,11 @@
 // pz_capi_frame.cu -- C ABI for ray queries, PathCache, photons, eye pass, work list,
 // plain specular solve and resolve (include/palzilla_b200.h).
 #include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
 
 #include "pz_batched_api.cuh"
 #include "pz_cache.cuh"
@@ -273,4 +278,181 @@ extern "C" int pz_resolve_spectral(float* rgb_dev, uint32_t* pixels_dev, const f
     return done(launch_resolve_spectral(reinterpret_cast<float4*>(rgb_dev), pixels_dev, spectral_dev, n_pixels, n_bins,
                                         lambda_min, lambda_max, F3(albedo), S(stream)),
                 "pz_resolve_spectral");
+}
+
+// ---------------------------------------------------------------- batches of scenes
+// Scratch: 256-byte header (status, work counter, record count, counters) | item offsets
+// (n_scenes + 1) | scene table | phase-1 records | probes, each region 256-byte aligned.
+namespace {
+constexpr size_t kMultiHeader = 256;
+inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+struct MultiLayout {
+    size_t offsets, table, records, probes, total;
+};
+MultiLayout multi_layout(int K, uint32_t nScenes, uint64_t maxPaths)
+{
+    MultiLayout L;
+    L.offsets = kMultiHeader;
+    L.table = L.offsets + align256(8 * ((size_t)nScenes + 1));
+    L.records = L.table + align256(sizeof(batched::SceneArgs) * (size_t)nScenes);
+    L.probes = L.records + align256((size_t)maxPaths * batched::record_bytes(K));
+    L.total = L.probes + align256((size_t)maxPaths * 3 * batched::probe_bytes(K));
+    return L;
+}
+
+// tunings found by pz_solve_multi_autotune, by (K, bins, log2 of the item capacity)
+std::mutex g_tune_mutex;
+std::map<std::tuple<int, int, int>, pz_batch_tuning> g_tunings;
+std::tuple<int, int, int> tune_key(int K, int nBins, uint64_t maxPaths)
+{
+    int lg = 0;
+    while ((1ull << lg) < maxPaths && lg < 63) lg++;
+    return std::make_tuple(K, nBins, lg);
+}
+}  // namespace
+
+extern "C" size_t pz_solve_multi_scratch_bytes(int K, uint32_t n_scenes, uint64_t max_paths_total)
+{
+    if (K < 1 || K > 4 || n_scenes == 0) return 0;
+    return multi_layout(K, n_scenes, max_paths_total).total;
+}
+
+extern "C" int pz_solve_multi_prepare(const pz_solve_desc* descs, const uint32_t* const* n_paths_dev, uint32_t n_scenes,
+                                      void* scratch_dev, size_t scratch_bytes, pz_stream_t stream)
+{
+    if (!descs || n_scenes == 0) return fail(PZ_ERR_INVALID_ARGUMENT, "pz_solve_multi_prepare: no scenes");
+    const int K = descs[0].K, nb = descs[0].n_bins;
+    uint64_t total = 0;
+    std::vector<batched::SceneArgs> table(n_scenes);
+    for (uint32_t i = 0; i < n_scenes; i++) {
+        const pz_solve_desc& d = descs[i];
+        if (d.K != K || d.n_bins != nb || !d.spectral || nb < 1 || nb > 64)
+            return fail(PZ_ERR_INVALID_ARGUMENT,
+                        "pz_solve_multi_prepare: scene %u: every scene needs the same K and 1..64 bins, binned mode", i);
+        int r = solve_args_from_desc(&d, &table[i].s, "pz_solve_multi_prepare");
+        if (r != PZ_OK) return r;
+        table[i].s.stats = nullptr;
+        table[i].nPathsDev = n_paths_dev ? n_paths_dev[i] : nullptr;
+        total += d.n_paths;
+    }
+    const MultiLayout L = multi_layout(K, n_scenes, total);
+    if (!scratch_dev || scratch_bytes < L.total)
+        return fail(PZ_ERR_SCRATCH_TOO_SMALL, "pz_solve_multi_prepare: scratch %zu < required %zu", scratch_bytes, L.total);
+    if (reinterpret_cast<uintptr_t>(scratch_dev) & 255)
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_solve_multi_prepare: scratch needs 256-byte alignment");
+    char* base = static_cast<char*>(scratch_dev);
+    cudaError_t e = cudaMemcpyAsync(base + L.table, table.data(), sizeof(batched::SceneArgs) * n_scenes,
+                                    cudaMemcpyHostToDevice, S(stream));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(S(stream));
+    return done(e, "pz_solve_multi_prepare");
+}
+
+static int multi_args(int K, int n_bins, uint32_t n_scenes, uint64_t total, void* scratch_dev, size_t scratch_bytes,
+                      unsigned long long* stats_dev, batched::BatchArgs* b, unsigned long long** offsets,
+                      const char* who)
+{
+    if (K < 1 || K > 4 || n_bins < 1 || n_bins > 64 || n_scenes == 0)
+        return fail(PZ_ERR_INVALID_ARGUMENT, "%s: bad K / bins / scene count", who);
+    const MultiLayout L = multi_layout(K, n_scenes, total);
+    if (!scratch_dev || scratch_bytes < L.total)
+        return fail(PZ_ERR_SCRATCH_TOO_SMALL, "%s: scratch %zu < required %zu", who, scratch_bytes, L.total);
+    char* base = static_cast<char*>(scratch_dev);
+    std::memset(&b->s, 0, sizeof(b->s));
+    b->s.nBins = n_bins;
+    b->s.stats = stats_dev;
+    b->status = reinterpret_cast<uint32_t*>(base);
+    b->workCounter = reinterpret_cast<unsigned long long*>(base + 8);
+    b->recordCount = reinterpret_cast<unsigned long long*>(base + 16);
+    b->counters = reinterpret_cast<unsigned long long*>(base + 64);
+    b->records = base + L.records;
+    b->recordCapacity = total;
+    b->probes = base + L.probes;
+    b->polishDet = 0.0;
+    b->continuation = 0;
+    b->illDet = 1.0e-2f;
+    b->scenes = reinterpret_cast<const batched::SceneArgs*>(base + L.table);
+    b->nScenes = n_scenes;
+    *offsets = reinterpret_cast<unsigned long long*>(base + L.offsets);
+    b->offsets = *offsets;
+    b->nPathsDev = nullptr;
+    return PZ_OK;
+}
+
+static cudaError_t run_multi(int K, const batched::BatchArgs& b0, const pz_batch_tuning& t, unsigned long long* offsets,
+                             void* scratch_dev, cudaStream_t s)
+{
+    batched::BatchArgs b = b0;
+    b.chunk = t.p2_chunk;
+    cudaError_t e = cudaMemsetAsync(scratch_dev, 0, kMultiHeader, s);
+    if (e == cudaSuccess) e = batched::launch_solve_batched_multi(K, b, t.p1_blocks_per_sm, t.p2_blocks_per_sm, offsets, s);
+    return e;
+}
+
+extern "C" int pz_solve_specular_multi(int K, int n_bins, uint32_t n_scenes, uint64_t max_paths_total,
+                                       void* scratch_dev, size_t scratch_bytes, const pz_batch_tuning* tuning,
+                                       unsigned long long* stats_dev, pz_stream_t stream)
+{
+    batched::BatchArgs b;
+    unsigned long long* offsets = nullptr;
+    int r = multi_args(K, n_bins, n_scenes, max_paths_total, scratch_dev, scratch_bytes, stats_dev, &b, &offsets,
+                       "pz_solve_specular_multi");
+    if (r != PZ_OK) return r;
+    pz_batch_tuning t = {8, 2, 1};
+    if (tuning) {
+        t = *tuning;
+    } else {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tunings.find(tune_key(K, n_bins, max_paths_total));
+        if (it != g_tunings.end()) t = it->second;
+    }
+    if (t.p1_blocks_per_sm < 1 || t.p1_blocks_per_sm > 32 || t.p2_blocks_per_sm < 1 || t.p2_blocks_per_sm > 2 ||
+        t.p2_chunk < 1 || t.p2_chunk > 64)
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_solve_specular_multi: tuning out of range");
+    return done(run_multi(K, b, t, offsets, scratch_dev, S(stream)), "pz_solve_specular_multi");
+}
+
+extern "C" int pz_solve_multi_autotune(int K, int n_bins, uint32_t n_scenes, uint64_t max_paths_total,
+                                       void* scratch_dev, size_t scratch_bytes, unsigned long long* stats_dev,
+                                       pz_batch_tuning* best_out, float* best_ms_out, pz_stream_t stream)
+{
+    batched::BatchArgs b;
+    unsigned long long* offsets = nullptr;
+    int r = multi_args(K, n_bins, n_scenes, max_paths_total, scratch_dev, scratch_bytes, stats_dev, &b, &offsets,
+                       "pz_solve_multi_autotune");
+    if (r != PZ_OK) return r;
+    cudaStream_t s = S(stream);
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+        return fail(PZ_ERR_CUDA, "pz_solve_multi_autotune: events");
+    pz_batch_tuning best = {8, 2, 1};
+    float bestMs = 3.4e38f;
+    cudaError_t e = run_multi(K, b, best, offsets, scratch_dev, s);  // warm-up
+    const int p1s[] = {4, 8, 16}, p2s[] = {1, 2}, chunks[] = {1, 4};
+    for (int p1 : p1s)
+        for (int p2 : p2s)
+            for (int c : chunks) {
+                if (e != cudaSuccess) break;
+                const pz_batch_tuning t = {p1, p2, c};
+                e = cudaEventRecord(e0, s);
+                if (e == cudaSuccess) e = run_multi(K, b, t, offsets, scratch_dev, s);
+                if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+                if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                float ms = 0.0f;
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+                if (e == cudaSuccess && ms < bestMs) {
+                    bestMs = ms;
+                    best = t;
+                }
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return cuda_fail(e, "pz_solve_multi_autotune");
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tunings[tune_key(K, n_bins, max_paths_total)] = best;
+    }
+    if (best_out) *best_out = best;
+    if (best_ms_out) *best_ms_out = bestMs;
+    clear_error();
+    return PZ_OK;
 }

@@ -273,9 +273,10 @@ def sphere_scene(subdivisions: int = 5, n_bins: int = 64, width: int = 1024, hei
                  events="TT", n_bins=n_bins, width=width, height=height)
 
 
-def uneven_batch(n_scenes: int = 256, seed: int = 3001, side_min: int = 16, side_max: int = 256):
+def uneven_batch(n_scenes: int = 256, seed: int = 3001, side_min: int = 16, side_max: int = 256, width: int = 256,
+                 height: int = 256, n_bins: int = 16, photons_per_triangle: int = 256):
     """Uneven batch: grid side log-uniform in [side_min, side_max], 1-2 refractions,
-    amplitude U[0.005, 0.03]."""
+    amplitude U[0.005, 0.03]; width x height receiver image and n_bins bins each."""
     rng = np.random.Generator(np.random.PCG64(seed))
     sides = np.exp(rng.uniform(math.log(side_min), math.log(side_max), n_scenes)).astype(int)
     amps = rng.uniform(0.005, 0.03, n_scenes)
@@ -283,6 +284,7 @@ def uneven_batch(n_scenes: int = 256, seed: int = 3001, side_min: int = 16, side
     scenes = []
     for i in range(n_scenes):
         s = lens_scene(int(sides[i]), seed=seed + 1 + i, amplitude=float(amps[i]), events="T" * int(ks[i]),
-                       n_bins=16, name=f"batch{i}")
+                       n_bins=n_bins, width=width, height=height, name=f"batch{i}")
+        s.photons_per_triangle = photons_per_triangle
         scenes.append(s)
     return scenes
