@@ -375,6 +375,124 @@ def bench_sort_build(hbm, hbm_kind, n=1 << 24):
                                "frac": build_gbs / hbm, "peak_kind": hbm_kind, "bytes_per_triangle": 261}}
 
 
+def run_uneven_batch(args):
+    """Uneven batch: 256 heightfield lenses (grid side log-uniform in 16..256, 450 to 130,050
+    triangles, 1-2 refractions, amplitude U[0.005, 0.03]), 256 x 256 image and 16 bins
+    each, 16 photons per triangle.  A frame renders every scene: eye pass, photon pass,
+    lookup / flatten with device item counts, the batched solve, resolve.  Three ways:
+    one batched solve per scene with the item count read back (the reference's host
+    flow), one batched solve per K over all scenes, and that frame captured in a CUDA
+    graph and replayed with the autotuned launch shapes."""
+    import torch
+    from palzilla_b200 import api as A
+    from palzilla_b200 import scenes as S
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    scenes = S.uneven_batch(n_scenes=args.batch_scenes, seed=3001, width=256, height=256, n_bins=16,
+                            photons_per_triangle=16)
+    items = []
+    for sc in scenes:
+        ds = A.DeviceScene(sc)
+        fr = A.Frame(sc, path_capacity=1 << 19)
+        # PathCache sized to the photon count (every photon inserts up to 8 cells)
+        cap = 1 << max(16, int(np.ceil(np.log2(4 * sc.n * sc.photons_per_triangle))))
+        items.append(dict(sc=sc, ds=ds, fr=fr, cache=A.PathCache(capacity=cap, step=sc.cell_step),
+                          ev=S.event_descriptor(sc.events), etas=torch.from_numpy(sc.bin_etas()).cuda(),
+                          spec=torch.zeros((sc.width * sc.height, sc.n_bins), device="cuda"),
+                          pixels=torch.zeros(sc.width * sc.height, dtype=torch.int32, device="cuda")))
+    stats = torch.zeros(3, dtype=torch.int64, device="cuda")
+
+    def size_work_list(it):
+        """One eye pass, photon pass and lookup; the work list then gets room for 1.25x the
+        item count it saw (the lookup counter counts past the capacity)."""
+        prep(it, 0, None)
+        n = int(it["fr"].counter.item())
+        need = 1 << max(16, int(np.ceil(np.log2(max(1, int(1.25 * n))))))
+        if need > it["fr"].path_capacity:
+            it["fr"] = A.Frame(it["sc"], path_capacity=need)
+
+    def prep(it, iteration, stream):
+        A.solve_primary(it["ds"], it["fr"], iteration=iteration, stream=stream)
+        it["cache"].clear(stream)
+        A.photon_trace(it["ds"], it["cache"], iteration=iteration, stream=stream)
+        it["fr"].counter.zero_()
+        A._lib.call("pz_lookup_flatten", A.C.c_uint32(it["ev"]), A._vp(it["fr"].paths), A._vp(it["fr"].indexed),
+                    A._vp(it["fr"].counter), A.C.c_uint32(it["fr"].path_capacity), A._vp(it["fr"].fd),
+                    A.C.c_int(it["fr"].npx), A._vp(it["cache"].buf), A.C.c_uint32(it["cache"].capacity),
+                    A.C.c_float(it["cache"].step), A.C.c_void_p(A._stream(stream)))
+        it["spec"].zero_()
+
+    def desc(it, cap):
+        return A.solve_desc(it["ds"], it["fr"], it["cache"], it["sc"].events, cap, spectral=it["spec"],
+                            etas=it["etas"])
+
+    for it in items:
+        size_work_list(it)
+    groups = {}
+    for it in items:
+        groups.setdefault(len(it["sc"].events), []).append(it)
+    batches = {K: A.SceneBatch([desc(it, it["fr"].path_capacity) for it in g], counts=[it["fr"].counter for it in g])
+               for K, g in groups.items()}
+
+    def frame_multi(iteration, stream=None, tuned=False):
+        for it in items:
+            prep(it, iteration, stream)
+        for K, sb in batches.items():
+            sb.solve(tuning=None if tuned else (8, 2, 1), stats=stats, stream=stream)
+        for it in items:
+            A.resolve_spectral(it["spec"], it["sc"], pixels=it["pixels"], stream=stream)
+
+    scratch = A.Scratch()
+
+    def frame_per_scene(iteration):
+        for it in items:
+            prep(it, iteration, None)
+            n = min(int(it["fr"].counter.item()), it["fr"].path_capacity)
+            d = desc(it, n)
+            d.stats = stats.data_ptr()
+            A.solve_specular_batched(d, scratch)
+            A.resolve_spectral(it["spec"], it["sc"], pixels=it["pixels"])
+
+    def timed(fn, k):
+        stats.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for i in range(k):
+            fn(i)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k, float(stats[0].item()) / k
+
+    for i in range(args.warmup):
+        frame_per_scene(i)
+        frame_multi(i)
+    tunings = {K: sb.autotune(stats=stats) for K, sb in batches.items()}
+    per_ms, paths = timed(frame_per_scene, args.steps)
+    multi_ms, paths_m = timed(frame_multi, args.steps)
+    stream = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        frame_multi(0, stream, tuned=True)  # warm the capture stream
+        torch.cuda.synchronize()
+        with torch.cuda.graph(graph, stream=stream):
+            frame_multi(0, stream, tuned=True)
+    graph_ms, paths_g = timed(lambda i: graph.replay(), args.steps)
+    tri = sum(it["sc"].n for it in items)
+    cache_status = sum(int(it["cache"].status() != 0) for it in items)
+    line = {"metric": "specular paths solved/s and ms/frame, uneven batch of scenes", "workload": "uneven_batch",
+            "path_cache_overflows": cache_status,
+            "value": paths_g / (graph_ms / 1e3), "unit": "paths/s", "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic", "scenes": len(items), "triangles": tri, "steps": args.steps, "warmup": args.warmup,
+            "path_solves_per_frame": paths_g,
+            "ms_per_frame": {"per_scene_solves": per_ms, "one_solve_per_K": multi_ms, "graph_autotuned": graph_ms},
+            "paths_per_s": {"per_scene_solves": paths / (per_ms / 1e3), "one_solve_per_K": paths_m / (multi_ms / 1e3),
+                            "graph_autotuned": paths_g / (graph_ms / 1e3)},
+            "tuning": {str(K): {"p1_blocks_per_sm": t[0][0], "p2_blocks_per_sm": t[0][1], "p2_chunk": t[0][2],
+                                "solve_ms": t[1]} for K, t in tunings.items()}}
+    print(json.dumps(line), flush=True)
+
+
 def run_sort_build(args):
     """Sort + build alone: n uniform random triangles (edges of 1e-3 to 1e-2), 32-bit Morton
     keys with 32-bit index payloads, onesweep sort and LBVH build, one line per size."""
@@ -485,12 +603,16 @@ def main():
     ap.add_argument("--ref-items", type=int, default=20000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-sort", action="store_true")
-    ap.add_argument("--workload", default="sphere", choices=["sphere", "sort_build"],
-                    help="sphere: the frame benchmark; sort_build: onesweep sort + LBVH build alone")
+    ap.add_argument("--workload", default="sphere", choices=["sphere", "sort_build", "uneven_batch"],
+                    help="sphere: the frame benchmark; sort_build: onesweep sort + LBVH build alone; "
+                         "uneven_batch: 256 heightfield lenses of uneven size per frame")
+    ap.add_argument("--batch-scenes", type=int, default=256)
     ap.add_argument("--sizes", default="20,22,24", help="log2 sizes of the sort_build workload")
     args = ap.parse_args()
     if args.workload == "sort_build":
         run_sort_build(args)
+    elif args.workload == "uneven_batch":
+        run_uneven_batch(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -261,9 +261,10 @@ struct SceneRef {
     uint64_t local;
     uint32_t scene;
 };
+template <bool kMulti>
 PZ_D SceneRef item_scene(const BatchArgs& a, uint64_t idx)
 {
-    if (!a.scenes) return SceneRef{&a.s, idx, 0u};
+    if (!kMulti) return SceneRef{&a.s, idx, 0u};
     uint32_t lo = 0, hi = a.nScenes;
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
@@ -272,9 +273,10 @@ PZ_D SceneRef item_scene(const BatchArgs& a, uint64_t idx)
     }
     return SceneRef{&a.scenes[lo].s, idx - a.offsets[lo], lo};
 }
+template <bool kMulti>
 PZ_D uint64_t total_items(const BatchArgs& a)
 {
-    if (a.scenes) return a.offsets[a.nScenes];
+    if (kMulti) return a.offsets[a.nScenes];
     return a.nPathsDev ? min((uint64_t)*a.nPathsDev, a.s.nPaths) : a.s.nPaths;
 }
 
@@ -314,17 +316,17 @@ __global__ void k_scene_offsets(const SceneArgs* scenes, uint32_t n, unsigned lo
 // One thread per (work item, probe bin): the plain path's solver from the photon's start at
 // the centre, first and last bin.  Kept apart from phase 1 so that it runs at the plain
 // kernel's occupancy; the three probes of an item sit in adjacent threads.
-template <int K>
+template <int K, bool kMulti>
 __global__ void __launch_bounds__(256) k_probe(BatchArgs a)
 {
     const int B = a.s.nBins;
-    const uint64_t nPaths = total_items(a);
+    const uint64_t nPaths = total_items<kMulti>(a);
     auto* probes = reinterpret_cast<Probe<K>*>(a.probes);
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < 3 * nPaths;
          t += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t idx = t / 3;
         const int q = (int)(t - 3 * idx);
-        const SceneRef R = item_scene(a, idx);
+        const SceneRef R = item_scene<kMulti>(a, idx);
         const SolveArgs& S = *R.s;
         const V3<float> L = v3f<float>(S.p_light);
         const SpecularPath sp = S.paths[R.local];
@@ -349,17 +351,17 @@ __global__ void __launch_bounds__(256) k_probe(BatchArgs a)
 }
 
 // ---------------------------------------------------------------- phase 1
-template <int K>
+template <int K, bool kMulti>
 __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
 {
     const int B = a.s.nBins;
-    const uint64_t nPaths = total_items(a);
+    const uint64_t nPaths = total_items<kMulti>(a);
     const int bc = B / 2;
     auto* recs = reinterpret_cast<PairRec<K>*>(a.records);
     unsigned long long nItems = 0;
     for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < nPaths;
          idx += (uint64_t)gridDim.x * blockDim.x) {
-        const SceneRef R = item_scene(a, idx);
+        const SceneRef R = item_scene<kMulti>(a, idx);
         const SolveArgs& S = *R.s;
         const float eta_c = S.etas[bc];
         const V3<float> L = v3f<float>(S.p_light);
@@ -521,7 +523,7 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
 }
 
 // ---------------------------------------------------------------- phase 2
-template <int K>
+template <int K, bool kMulti>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
 {
     __shared__ uint32_t cand[kWarpsPerBlock][kMaxCand];
@@ -541,7 +543,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
         }
         if (j >= nRec) break;
         const PairRec<K> r = recs[j++];
-        const SolveArgs& S = a.scenes ? a.scenes[r.scene].s : a.s;
+        const SolveArgs& S = kMulti ? a.scenes[r.scene].s : a.s;
         const uint32_t root = __ldg(S.root);
         const float eta_c = S.etas[B / 2];
         const V3<float> L = v3f<float>(S.p_light);
@@ -679,9 +681,15 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
 template <int K>
 static cudaError_t launch_k(const BatchArgs& a, int blocksPerSM, cudaStream_t s, int p1BlocksPerSM = 8)
 {
-    k_probe<K><<<kNumSMs * 2 * p1BlocksPerSM, 256, 0, s>>>(a);
-    k_phase1<K><<<kNumSMs * p1BlocksPerSM, 256, 0, s>>>(a);
-    k_phase2<K><<<kNumSMs * blocksPerSM, kWarpsPerBlock * 32, 0, s>>>(a);
+    if (a.scenes) {
+        k_probe<K, true><<<kNumSMs * 2 * p1BlocksPerSM, 256, 0, s>>>(a);
+        k_phase1<K, true><<<kNumSMs * p1BlocksPerSM, 256, 0, s>>>(a);
+        k_phase2<K, true><<<kNumSMs * blocksPerSM, kWarpsPerBlock * 32, 0, s>>>(a);
+    } else {
+        k_probe<K, false><<<kNumSMs * 2 * p1BlocksPerSM, 256, 0, s>>>(a);
+        k_phase1<K, false><<<kNumSMs * p1BlocksPerSM, 256, 0, s>>>(a);
+        k_phase2<K, false><<<kNumSMs * blocksPerSM, kWarpsPerBlock * 32, 0, s>>>(a);
+    }
     return cudaGetLastError();
 }
 
