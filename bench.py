@@ -493,6 +493,102 @@ def run_uneven_batch(args):
     print(json.dumps(line), flush=True)
 
 
+def run_pathcuts(args):
+    """Path Cuts (traverseAdmissibleNodes<2>, TT) on the two-sheet heightfield lens (side 64:
+    8,388 triangles, USE_NORMAL BVH): admissible tuples of 4,096 receiver points on a grid,
+    round-to-nearest and directed rounding; the reference's CPU traversal (oracle/_ref) is
+    timed on a bounded sample of the points (one OpenMP thread per query)."""
+    import torch
+    from palzilla_b200 import api as A
+    from palzilla_b200 import scenes as S
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    sc = S.lens_scene(side=64, seed=1, width=64, height=64, n_bins=1, events="TT")
+    t = torch.from_numpy(np.ascontiguousarray(sc.tris)).cuda()
+    at = torch.from_numpy(np.ascontiguousarray(sc.attribs).view(np.uint8).reshape(-1)).cuda()
+    b = A.BVHGPUBuilder()
+    b.build(t, sc.n, 1)
+    nbs = A.normal_bounds(b, at)
+    g = np.linspace(-0.45, 0.45, 64, dtype=np.float32)
+    X, Z = np.meshgrid(g, g)
+    ends = np.stack([X.ravel(), np.zeros(X.size, np.float32), Z.ravel()], 1).astype(np.float32)
+    ends_d = torch.from_numpy(ends).cuda()
+    pc = A.PathCuts(frontier_capacity=1 << 26, tuple_capacity=1 << 25)
+    ev = S.event_descriptor("TT")
+    res = {}
+    for mode in ("rn", "dr"):
+        for i in range(args.warmup):
+            pc.run(2, ev, 1.52, sc.p_light, ends_d, b, nbs, t, at, directed=mode == "dr")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i in range(args.steps):
+            rows, visited = pc.run(2, ev, 1.52, sc.p_light, ends_d, b, nbs, t, at, directed=mode == "dr")
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3 / args.steps
+        res[mode] = {"ms": ms, "tuples": int(rows.shape[0]), "node_tuples": int(visited),
+                     "node_tuples_per_s": visited / (ms / 1e3), "queries_per_s": len(ends) / (ms / 1e3)}
+    cpu = None
+    lib, kind = _cpu_lib()
+    if lib.has("path_cuts"):
+        import oracle as O
+        bo = lib.build_bvh(sc.tris, 1)
+        nbo = lib.normal_bounds(bo["nodes"], sc.tris, sc.attribs)
+        sample = ends[:: max(1, len(ends) // args.cuts_sample)]
+        t0 = time.perf_counter()
+        n_cpu = 0
+        for pe in sample:
+            n_cpu += len(lib.path_cuts(2, ev, 1.52, sc.p_light, pe, bo["nodes"], nbo, sc.tris, sc.attribs, bo["root"]))
+        dt = time.perf_counter() - t0
+        cpu = {"value": len(sample) / dt, "unit": "queries/s", "cores": 1, "kind": kind,
+               "sample": f"{len(sample)} of the {len(ends)} receiver points, {n_cpu} tuples, {dt:.1f} s"}
+    print(json.dumps({"metric": "Path Cuts queries/s (admissible K=2 tuples per receiver point)",
+                      "workload": "pathcuts", "value": res["rn"]["queries_per_s"], "unit": "queries/s",
+                      "higher_is_better": True, "data": "synthetic", "triangles": sc.n, "queries": len(ends),
+                      "round_to_nearest": res["rn"], "directed_rounding": res["dr"], "cpu_baseline": cpu}),
+          flush=True)
+
+
+def run_adjoint(args):
+    """Adjoint workload: 128 x 128 heightfield lens (32,258 triangles), 512 x 512 image, 8
+    bins, L2 loss against a second seeded heightfield: forward (exact-arithmetic binned
+    solve) and backward (roots recomputed, implicit-function gradients) per step."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from grad_harness import CausticProblem
+    from palzilla_b200 import scenes as S
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    sc, corners, h0 = S.adjoint_scene(side=128, seed=1)
+    P = CausticProblem(sc, corners)
+    sc2, c2, h2 = S.adjoint_scene(side=128, seed=2)
+    P2 = CausticProblem(sc2, c2)
+    cauchy = torch.tensor([1.5, 4200.0], dtype=torch.float32, device="cuda")
+    target = P2.forward(torch.from_numpy(h2).cuda(), cauchy).clone()
+    del P2
+    h = torch.from_numpy(h0).cuda()
+    for i in range(args.warmup):
+        I = P.forward(h, cauchy)
+        P.backward(h, cauchy, (2.0 * (I - target)).contiguous())
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    fwd, bwd = [], []
+    for i in range(args.steps):
+        ev[0].record()
+        I = P.forward(h, cauchy)
+        ev[1].record()
+        gh, gc = P.backward(h, cauchy, (2.0 * (I - target)).contiguous())
+        ev[2].record()
+        torch.cuda.synchronize()
+        fwd.append(ev[0].elapsed_time(ev[1]))
+        bwd.append(ev[1].elapsed_time(ev[2]))
+    paths = P.n_paths * sc.n_bins
+    print(json.dumps({"metric": "adjoint forward + backward ms (gradient of an L2 image loss)",
+                      "workload": "adjoint", "value": float(np.mean(fwd) + np.mean(bwd)), "unit": "ms",
+                      "higher_is_better": False, "data": "synthetic", "triangles": sc.n, "image": "512x512x8",
+                      "path_solves": paths, "forward_ms": float(np.mean(fwd)), "backward_ms": float(np.mean(bwd)),
+                      "backward_paths_per_s": paths / (float(np.mean(bwd)) / 1e3),
+                      "note": "forward includes the LBVH rebuild from the heights; backward includes it too"}),
+          flush=True)
+
+
 def run_sort_build(args):
     """Sort + build alone: n uniform random triangles (edges of 1e-3 to 1e-2), 32-bit Morton
     keys with 32-bit index payloads, onesweep sort and LBVH build, one line per size."""
@@ -603,16 +699,22 @@ def main():
     ap.add_argument("--ref-items", type=int, default=20000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-sort", action="store_true")
-    ap.add_argument("--workload", default="sphere", choices=["sphere", "sort_build", "uneven_batch"],
+    ap.add_argument("--workload", default="sphere", choices=["sphere", "sort_build", "uneven_batch", "pathcuts",
+                                                             "adjoint"],
                     help="sphere: the frame benchmark; sort_build: onesweep sort + LBVH build alone; "
                          "uneven_batch: 256 heightfield lenses of uneven size per frame")
     ap.add_argument("--batch-scenes", type=int, default=256)
+    ap.add_argument("--cuts-sample", type=int, default=64)
     ap.add_argument("--sizes", default="20,22,24", help="log2 sizes of the sort_build workload")
     args = ap.parse_args()
     if args.workload == "sort_build":
         run_sort_build(args)
     elif args.workload == "uneven_batch":
         run_uneven_batch(args)
+    elif args.workload == "pathcuts":
+        run_pathcuts(args)
+    elif args.workload == "adjoint":
+        run_adjoint(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -239,6 +239,18 @@ __device__ __noinline__ float dadw_out_of_line(const Chain<K>& ch, const float* 
 #endif
 }
 
+// Newton on the multi-tangent Jacobian, out of line: one copy of the body serves every
+// call site (the kernels are instruction-cache bound when it is inlined several times).
+template <int K>
+__device__ __noinline__ bool newton_nl(float* x, const Chain<K>& ch, float3 p_light, float3 p, float eta,
+                                       uint32_t events, int maxIterations, float tol, int warmup, bool edge,
+                                       int minSteps, float* det)
+{
+    int it;
+    return newton<float, K>(x, v3f<float>(p_light), v3f<float>(p), ch, eta, events, maxIterations, tol, warmup, edge,
+                            &it, det, minSteps);
+}
+
 // The plain path's solve (solveConstraints' rules from the photon's start: cost tolerance,
 // edge rejection after the warm-up iterations) on the multi-tangent Jacobian, whose
 // columns follow the reference's single-tangent operation order.  Out of line: phase 2
@@ -247,10 +259,8 @@ template <int K>
 __device__ __noinline__ bool plain_solve(float* x, const Chain<K>& ch, float3 p_light, float3 p, float eta,
                                          uint32_t events, int maxIterations, float tol, int warmup)
 {
-    int it;
     float det;
-    return newton<float, K>(x, v3f<float>(p_light), v3f<float>(p), ch, eta, events, maxIterations, tol, warmup, true,
-                            &it, &det, 0);
+    return newton_nl<K>(x, ch, p_light, p, eta, events, maxIterations, tol, warmup, true, 0, &det);
 }
 
 // ---------------------------------------------------------------- scenes of a batch
@@ -340,10 +350,9 @@ __global__ void __launch_bounds__(256) k_probe(BatchArgs a)
 #pragma unroll
         for (int i = 0; i < 2 * K; i++) r.x[i] = pp[i];
         const int b = q == 0 ? B / 2 : (q == 1 ? 0 : B - 1);
-        int it;
         float det;
-        r.ok = newton<float, K>(r.x, L, v3f<float>(S.fds[sp.pixel].p), ch, S.etas[b], S.events, S.maxIterations,
-                                S.costTolerance, S.earlyTermWarmUp, true, &it, &det, 0)
+        r.ok = newton_nl<K>(r.x, ch, S.p_light, S.fds[sp.pixel].p, S.etas[b], S.events, S.maxIterations,
+                            S.costTolerance, S.earlyTermWarmUp, true, 0, &det)
                    ? 1u
                    : 0u;
         probes[t] = r;
@@ -376,7 +385,6 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
 #pragma unroll
         for (int i = 0; i < 2 * K; i++) x[i] = xpc[i] = pp[i];
         const V3<float> p = v3f<float>(S.fds[sp.pixel].p);
-        int it;
         float det = 1.0f;
         // the plain path's decision at the centre bin (k_probe); when it converged, its root
         // is the branch followed below
@@ -389,7 +397,8 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
 #pragma unroll
             for (int i = 0; i < 2 * K; i++) x[i] = xpc[i];
         } else {
-            conv = newton<float, K>(x, L, p, ch, eta_c, S.events, 24, S.costTolerance, 0, false, &it, &det);
+            conv = newton_nl<K>(x, ch, S.p_light, S.fds[sp.pixel].p, eta_c, S.events, 24, S.costTolerance, 0, false, 0,
+                                &det);
         }
         PairRec<K> r;
         r.pixel = sp.pixel;
@@ -423,12 +432,11 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
                 r.xa[i] = lin_a[i];
                 r.xb[i] = lin_b[i];
             }
-            int ia, ib;
             float da, db;
             const bool ca =
-                newton<float, K>(r.xa, L, p, ch, ea, S.events, 12, S.costTolerance, 0, false, &ia, &da, 1);
+                newton_nl<K>(r.xa, ch, S.p_light, S.fds[sp.pixel].p, ea, S.events, 12, S.costTolerance, 0, false, 1, &da);
             const bool cb =
-                newton<float, K>(r.xb, L, p, ch, eb, S.events, 12, S.costTolerance, 0, false, &ib, &db, 1);
+                newton_nl<K>(r.xb, ch, S.p_light, S.fds[sp.pixel].p, eb, S.events, 12, S.costTolerance, 0, false, 1, &db);
             float nonlin = 0.0f;
             bool finite = true;
 #pragma unroll
@@ -583,14 +591,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
 #pragma unroll
                     for (int i = 0; i < 2 * K; i++) xs[i] = x0[i];
                 }
-                int it;
                 float det = 1.0f;
                 // a predicted root is refined by Newton; every other bin runs the plain path's
                 // solver from the photon's start, so its accept / reject decision is the plain one
-                const bool conv = warm ? newton<float, K>(xs, L, p, ch, eta, S.events, S.maxIterations,
-                                                          S.costTolerance, S.earlyTermWarmUp, true, &it, &det, 1)
-                                       : plain_solve<K>(xs, ch, S.p_light, fd.p, eta, S.events, S.maxIterations,
-                                                        S.costTolerance, S.earlyTermWarmUp);
+                const bool conv = newton_nl<K>(xs, ch, S.p_light, fd.p, eta, S.events, S.maxIterations,
+                                               S.costTolerance, S.earlyTermWarmUp, true, warm ? 1 : 0, &det);
                 if (a.counters) atomicAdd(a.counters + kCntNewton2, 1ull);
                 if (conv) {
                     nConv++;
