@@ -47,9 +47,9 @@ WORKLOAD = {
 # kernels of this library launched per frame: k_primary, k_photon, k_lookup, sort k_hist + 4 x k_pass,
 # k_reorder, k_probe, k_phase1, k_phase2, k_resolve_spectral
 LAUNCHES_PER_FRAME = 13
-# DRAM bytes (read + write) per work item of k_phase1 + k_phase2, from one ncu capture of the
-# first frame of this workload (profiles/sphere_solver_photon_kernels.md): 3411.8 MB / 19.8 M items
-NCU_SOLVE_TRAFFIC_PER_ITEM = 172.3
+# DRAM bytes (read + write) per work item of k_probe + k_phase1 + k_phase2, from one ncu capture
+# of the first frame of this workload (profiles/sphere_solver_kernels.md): 6322.5 MB / 19.8 M items
+NCU_SOLVE_TRAFFIC_PER_ITEM = 319.3
 
 
 def peaks():
@@ -290,7 +290,8 @@ def run_ours(args):
     # + two triangles 72 + two attributes 80 = 248 B read once; 4 B per contributing (item, bin) added
     alg_bytes = n_items * 248.0 + contributing * 4.0
     achieved = alg_bytes / (solve_avg / 1e3) / 1e9
-    roofline = {"kernel": "k_phase1 + k_phase2 (batched solve)", "bound": "hbm", "achieved": achieved, "peak": hbm,
+    roofline = {"kernel": "k_probe + k_phase1 + k_phase2 (batched solve)", "bound": "hbm", "achieved": achieved,
+                "peak": hbm,
                 "unit": "GB/s", "frac": achieved / hbm, "peak_kind": hbm_kind,
                 "traffic": NCU_SOLVE_TRAFFIC_PER_ITEM * n_items if NCU_SOLVE_TRAFFIC_PER_ITEM else None,
                 "algorithmic_bytes": alg_bytes,
