@@ -39,7 +39,8 @@ METRIC = "specular paths solved/s and ms/frame, batched vs plain GPU at 1e-3 ima
 UNIT = "paths/s"
 WORKLOAD = {
     "workload": "two-refraction dispersive sphere",
-    "triangles": 20480, "scene": "icosphere-5 r=0.5 at (0,1,0), 4x4 receiver at y=0, light (0,4,0)",
+    "triangles": 20480, "scene": "icosphere-5 r=0.5 at (0,1,0), 4x4 receiver at y=0",
+    "light": "0.2x0.2 area light centred at (0,4,0), one point sample per frame (R2 sequence)",
     "ior": "cauchy 1.5 + 4200/nm^2", "image": "1024x1024", "bins": 64, "lambda_nm": [380, 780],
     "photons": 20480 * 205, "events": "TT", "path_cache": 1 << 22,
     "l2": "no flush: every frame streams buffers larger than L2 (PathCache 252 MB, spectral image 268 MB)",
@@ -172,10 +173,13 @@ class Renderer:
         self.pixels = torch.zeros(npx, dtype=torch.int32, device="cuda")
         self.stats = torch.zeros(3, dtype=torch.int64, device="cuda")
         self.n_paths = 0
+        self.iteration = 0
 
     def prepare(self, iteration: int):
-        """Eye pass, photon pass, lookup/flatten (count read back), sort and reorder."""
+        """Eye pass, photon pass, lookup/flatten (count read back), sort and reorder, with
+        the light point of this iteration (one sample of the area light)."""
         A, fr = self.A, self.frame
+        self.iteration = iteration
         A.solve_primary(self.ds, fr, iteration=iteration)
         self.cache.clear()
         A.photon_trace(self.ds, self.cache, iteration=iteration)
@@ -187,7 +191,7 @@ class Renderer:
         A, sc = self.A, self.sc
         self.spectral.zero_()
         d = A.solve_desc(self.ds, self.frame, self.cache, sc.events, self.n_paths, spectral=self.spectral,
-                         etas=self.etas, stats=self.stats, exact=exact)
+                         etas=self.etas, stats=self.stats, exact=exact, iteration=self.iteration)
         if solve_events:
             solve_events[0].record()
         if plain:

@@ -305,6 +305,67 @@ PZ_API int pz_path_cuts(int K, uint32_t events, float eta, pz_float3 p_beg, cons
                         uint64_t* n_tuples_out, uint64_t* node_tuples_out, void* scratch_dev, size_t scratch_bytes,
                         pz_stream_t stream);
 
+/* ---------------------------------------------------------------- subdivision solve
+ * No reference counterpart (the reference solves each admissible tuple once, from one
+ * start: main.cpp:1052).  For every tuple row {q, triangle[0..K)} -- the rows pz_path_cuts
+ * writes -- the domain of the 2K barycentrics is bisected (split t halves dimension
+ * t mod 2K) under affine bounds of the specular constraint of solveConstraints<K>
+ * (pk.h:466-592) with rounding-error terms rounded upward; boxes whose bound excludes
+ * zero, that lie outside a triangle or whose cosines rule the event out are dropped.
+ * A box stops splitting at max_depth, or when every bounded residual component is
+ * narrower than eps; its centre starts the Newton solve for each wavelength bin
+ * (eta = etas_dev[bin]; the bins share one subdivision).  A root is kept when it
+ * converged, lies in its own box (each root has one owner box) and
+ * contributableThroughput (pk.h:760-842) is positive.  The tuple rows index
+ * triangles_dev / attribs_dev (the specular soup pz_path_cuts ran on, or the scene);
+ * visibility runs through the scene's BVH (scene_internals_dev, scene_triangles_dev,
+ * scene_root_dev). */
+typedef struct pz_subdiv_params {
+    int max_depth;         /* 12: bisections of a tuple's domain (0..20) */
+    float eps;             /* 1e-4: residual width at which a box stops splitting */
+    int max_iterations;    /* 32 (main_gpu.cu:456) */
+    float cost_tolerance;  /* 1e-10 */
+    int early_term_warmup; /* 1 */
+    int fp64_polish;       /* 0; 1 = 4 FP64 Newton steps on every root found in its box */
+} pz_subdiv_params;
+typedef struct pz_subdiv_stats {
+    uint64_t boxes_tested, boxes_culled, leaves, solves, converged, outside_box, roots, polished;
+} pz_subdiv_stats;
+typedef struct pz_specular_root {
+    uint32_t tuple;   /* row of tuples_dev */
+    uint32_t bin;     /* wavelength bin */
+    uint32_t depth;   /* owner box: depth ... */
+    uint32_t path;    /* ... and bisection path (bit t = half taken at split t) */
+    float params[8];  /* barycentrics (u, v) per vertex; 2K used */
+    float throughput; /* contributableThroughput, > 0 */
+    uint32_t pad[3];
+} pz_specular_root;   /* 64 bytes */
+/* Scratch: a 256-byte header, two box frontiers and the leaf list of box_capacity entries
+ * each (box_capacity >= n_tuples). */
+PZ_API size_t pz_subdivide_scratch_bytes(uint64_t box_capacity);
+/* Writes the kept roots (unordered) to roots_dev and their count (which may exceed
+ * root_capacity: PZ_ERR_DEVICE is then returned) to *n_roots_out.  Synchronises `stream`
+ * once, at the end. */
+PZ_API int pz_subdivide_solve(int K, uint32_t events, pz_float3 p_beg, const pz_float3* p_end_dev,
+                              const uint32_t* tuples_dev, uint32_t n_tuples, const float* etas_dev, int n_bins,
+                              const pz_subdiv_params* params, const pz_triangle* triangles_dev,
+                              const pz_triangle_attrib* attribs_dev, const pz_internal_node* scene_internals_dev,
+                              const pz_triangle* scene_triangles_dev, const uint32_t* scene_root_dev,
+                              pz_specular_root* roots_dev, uint64_t root_capacity, uint64_t* n_roots_out,
+                              pz_subdiv_stats* stats_out, void* scratch_dev, size_t scratch_bytes,
+                              pz_stream_t stream);
+/* The roots' contributions to a binned spectral image (spectral_dev: n_pixels x n_bins
+ * floats, accumulated): the tail of solveSpecularPath<K> (main_gpu.cu:466-486) with the
+ * wavelength fixed to each root's bin -- throughput * light_intensity / dAdw * cos at the
+ * receiver, clamped at radiance_clamp.  The tuple rows' query index is the pixel of
+ * first_diffuse_dev (pz_solve_primary's FirstDiffuse records; the solve's p_end of a
+ * query is that pixel's receiver point).  Triangles as for pz_subdivide_solve. */
+PZ_API int pz_subdivide_contribute(int K, uint32_t events, pz_float3 p_beg, float light_intensity,
+                                   float radiance_clamp, const uint32_t* tuples_dev,
+                                   const pz_specular_root* roots_dev, uint64_t n_roots, const void* first_diffuse_dev,
+                                   const float* etas_dev, int n_bins, const pz_triangle* triangles_dev,
+                                   const pz_triangle_attrib* attribs_dev, float* spectral_dev, pz_stream_t stream);
+
 /* ---------------------------------------------------------------- adjoint
  * No reference counterpart.  A forward / backward pair for gradients of a loss on the
  * binned spectral image.  Forward: the plain binned solve in the reference's arithmetic

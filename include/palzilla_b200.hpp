@@ -12,6 +12,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -159,6 +160,20 @@ struct RayGenerator {
     }
 };
 
+// No reference counterpart (the reference has a point light).  Sample `iteration` of a
+// downward-facing square light of extent (size_x, size_z) centred on `center`: the R2
+// sequence (Roberts 2018: x_i = frac(1/2 + i / g), y_i = frac(1/2 + i / g^2), g the
+// plastic number), in double, rounded to float.  Iteration 0 is the centre; a light of
+// size zero is its centre.
+inline pz_float3 light_point(pz_float3 center, float size_x, float size_z, int iteration)
+{
+    if (size_x == 0.0f && size_z == 0.0f) return center;
+    const double g = 1.32471795724474602596;
+    const double u = std::fmod(0.5 + iteration / g, 1.0), v = std::fmod(0.5 + iteration / (g * g), 1.0);
+    return pz_float3{(float)((double)center.x + (u - 0.5) * (double)size_x), center.y,
+                     (float)((double)center.z + (v - 0.5) * (double)size_z)};
+}
+
 // The reference's event descriptor (pk.h:122-162): bit k set = transmission at vertex k.
 inline uint32_t event_descriptor(const std::string& events)
 {
@@ -172,6 +187,7 @@ class PKRenderer {
 public:
     // tunables, as the reference's members (pk.h:1683-1701)
     pz_float3 m_p_light = {0.0f, 3.0f, 0.0f};
+    float m_lightSize[2] = {0.0f, 0.0f};  // area light extent along x and z (0: point light)
     float m_lightIntencity = 16.0f;
     float m_minThroughput = 0.05f;
     float m_radianceClamp = 12.0f;
@@ -221,9 +237,10 @@ public:
     {
         cudaStream_t s = 0;
         const int n = m_gpuBuilder.m_nTriangles;
+        m_lightPoint = light_point(m_p_light, m_lightSize[0], m_lightSize[1], m_iteration);
         check(pz_solve_primary(m_accumulators.data(), m_firstDiffuses.data(), m_imageWidth, m_imageHeight, &m_camera.g,
                                &m_lensParams, m_gpuBuilder.m_internals, m_gpuBuilder.m_rootNode,
-                               m_trianglesDevice.data(), m_triangleAttribsDevice.data(), m_p_light, m_lightIntencity,
+                               m_trianglesDevice.data(), m_triangleAttribsDevice.data(), m_lightPoint, m_lightIntencity,
                                m_radianceClamp, m_cauchyA, m_cauchyB, m_albedo, m_iteration, m_status.data(),
                                (pz_stream_t)s),
               "solvePrimary");
@@ -232,7 +249,7 @@ public:
         const float etaMin = m_cauchyA + m_cauchyB / (380.0f * 380.0f);
         const float etaMax = m_cauchyA + m_cauchyB / (780.0f * 780.0f);
         check(pz_photon_trace(m_gpuBuilder.m_internals, m_gpuBuilder.m_rootNode, m_trianglesDevice.data(),
-                              m_triangleAttribsDevice.data(), n, m_photonsPerTriangle, m_p_light, etaMin, etaMax,
+                              m_triangleAttribsDevice.data(), n, m_photonsPerTriangle, m_lightPoint, etaMin, etaMax,
                               m_iteration, m_minThroughput, m_pathCache.data(), kPathCacheCapacity, kCellStep, nullptr,
                               (pz_stream_t)s),
               "photonTrace");
@@ -259,6 +276,7 @@ public:
 private:
     static constexpr uint32_t kPathCacheCapacity = 1u << 22;
     static constexpr float kCellStep = 0.01f;
+    pz_float3 m_lightPoint = {0.0f, 0.0f, 0.0f};  // the light's sample for the current step
 
     void solveSpecular(const char* events)
     {
@@ -293,7 +311,7 @@ private:
         d.cache = m_pathCache.data();
         d.cache_capacity = kPathCacheCapacity;
         d.cell_step = kCellStep;
-        d.p_light = m_p_light;
+        d.p_light = m_lightPoint;
         d.light_intensity = m_lightIntencity;
         d.radiance_clamp = m_radianceClamp;
         d.cauchy_a = m_cauchyA;

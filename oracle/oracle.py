@@ -27,15 +27,24 @@ NODE_DTYPE = np.dtype([("children", "<u4", (2,)), ("aabbs", "<f4", (2, 6)), ("pa
 assert NODE_DTYPE.itemsize == 64
 NORMAL_BOUND_DTYPE = np.dtype([("bounds", "<f4", (2, 6)), ("counter", "<u4")])
 assert NORMAL_BOUND_DTYPE.itemsize == 52
+ROOT_DTYPE = np.dtype([("tuple", "<u4"), ("bin", "<u4"), ("depth", "<u4"), ("path", "<u4"), ("params", "<f4", (8,)),
+                       ("throughput", "<f4"), ("pad", "<u4", (3,))])
+assert ROOT_DTYPE.itemsize == 64
 RECORD_DTYPE = np.dtype([("ev", "<u4"), ("tris", "<i4", (4,)), ("params", "<f4", (8,)), ("p", "<f4", (3,))])
 assert RECORD_DTYPE.itemsize == 64
 INVALID_NODE = 0x7FFFFFFF
 
 
+def _light(scene, iteration: int) -> np.ndarray:
+    """The scene's light point at this iteration (one sample of an area light)."""
+    p = scene.light_point(iteration) if hasattr(scene, "light_point") else scene.p_light
+    return np.asarray(p, np.float32)
+
+
 def build_oracle(force: bool = False) -> None:
     """Compile the restatement library (make in oracle/)."""
     if force or not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < max(
-            os.path.getmtime(os.path.join(HERE, f)) for f in ("pz_oracle.hpp", "pz_oracle_capi.cpp")):
+            os.path.getmtime(os.path.join(HERE, f)) for f in ("pz_oracle.hpp", "pz_oracle_subdiv.hpp", "pz_oracle_capi.cpp")):
         subprocess.run(["make", "-C", HERE, "-s"], check=True)
 
 
@@ -151,7 +160,7 @@ class CpuLib:
         emin, emax = eta_range or scene.eta_range()
         n = self.f("photon_trace", C.c_int64)(
             _p(bvh["nodes"]), C.c_uint32(bvh["root"]), _p(scene.tris), _p(scene.attribs), C.c_int(scene.n),
-            _p(np.asarray(scene.p_light, np.float32)), C.c_float(emin), C.c_float(emax), C.c_int(iteration),
+            _p(_light(scene, iteration)), C.c_float(emin), C.c_float(emax), C.c_int(iteration),
             C.c_float(scene.min_throughput), C.c_int(ppt), _p(out), C.c_int64(cap))
         if n < 0:
             raise RuntimeError("photon record capacity exceeded")
@@ -196,7 +205,7 @@ class CpuLib:
         fd = np.zeros((H * W, 10), np.float32)
         self.f("solve_primary")(_p(accum), _p(fd), C.c_int(W), C.c_int(H), _p(np.asarray(ray_gen, np.float32)),
                                 _p(np.asarray(lens, np.float32)), _p(bvh["nodes"]), C.c_uint32(bvh["root"]),
-                                _p(scene.tris), _p(scene.attribs), _p(np.asarray(scene.p_light, np.float32)),
+                                _p(scene.tris), _p(scene.attribs), _p(_light(scene, iteration)),
                                 C.c_float(scene.light_intensity), C.c_float(scene.radiance_clamp),
                                 C.c_float(scene.cauchy_a), C.c_float(scene.cauchy_b),
                                 _p(np.asarray(scene.albedo, np.float32)), C.c_int(iteration))
@@ -249,7 +258,7 @@ class CpuLib:
             C.c_float(eta)))
 
     def render_pairs(self, K, pairs, cache, first_diffuse, bvh, scene, etas, max_iter=32, tol=1e-10, warmup=1,
-                     dtype=np.float32):
+                     dtype=np.float32, iteration=0):
         pairs = np.ascontiguousarray(pairs, np.int32)
         etas = np.ascontiguousarray(etas, np.float32)
         nb = etas.size
@@ -264,14 +273,14 @@ class CpuLib:
             args.append(C.c_int(0 if dtype == np.float32 else 1))
         args += [_p(pairs), C.c_int64(pairs.shape[0]), _p(cache["tris"]), _p(cache["params"]),
                  _p(np.ascontiguousarray(first_diffuse, np.float32)), _p(bvh["nodes"]), C.c_uint32(bvh["root"]),
-                 _p(scene.tris), _p(scene.attribs), _p(np.asarray(scene.p_light, np.float32)),
+                 _p(scene.tris), _p(scene.attribs), _p(_light(scene, iteration)),
                  C.c_float(scene.light_intensity), C.c_float(scene.radiance_clamp), C.c_uint32(ev), _p(etas),
                  C.c_int(nb), C.c_int(max_iter), C.c_float(tol), C.c_int(warmup), _p(spectral), _p(stats)]
         self.f("render_pairs", C.c_int)(*args)
         return spectral, stats
 
     def render_each(self, K, pairs, cache, first_diffuse, bvh, scene, etas, max_iter=32, tol=1e-10, warmup=1,
-                    dtype=np.float64):
+                    dtype=np.float64, iteration=0):
         """Contribution of every (pair, bin) before the clamp (0 = rejected), (n_pairs, n_bins) float64."""
         pairs = np.ascontiguousarray(pairs, np.int32)
         etas = np.ascontiguousarray(etas, np.float32)
@@ -281,7 +290,7 @@ class CpuLib:
             C.c_int(K), C.c_int(0 if dtype == np.float32 else 1), _p(pairs), C.c_int64(pairs.shape[0]),
             _p(cache["tris"]), _p(cache["params"]), _p(np.ascontiguousarray(first_diffuse, np.float32)),
             _p(bvh["nodes"]), C.c_uint32(bvh["root"]), _p(scene.tris), _p(scene.attribs),
-            _p(np.asarray(scene.p_light, np.float32)), C.c_float(scene.light_intensity),
+            _p(_light(scene, iteration)), C.c_float(scene.light_intensity),
             C.c_uint32(event_descriptor(scene.events)), _p(etas), C.c_int(etas.size), C.c_int(max_iter),
             C.c_float(tol), C.c_int(warmup), _p(out))
         return out
@@ -324,6 +333,44 @@ class CpuLib:
         if n < 0:
             raise RuntimeError("tuple capacity exceeded")
         return out[:n].copy()
+
+    # ------------------------------------------------------------------ subdivision solve
+    def subdivide_solve(self, K, ev, p_beg, p_end, tuples, etas, tris, attribs, bvh, scene_tris, max_depth=12,
+                        eps=1e-4, max_iterations=32, cost_tolerance=1e-10, warm_up=1, cap=1 << 20):
+        """Roots of the subdivision solve, sorted by (tuple, bin, depth, path), and the stats
+        (tested, culled, leaves, solves, converged, outside, roots).  tuples index
+        tris / attribs; visibility runs through bvh over scene_tris."""
+        tuples = np.ascontiguousarray(tuples, np.uint32)
+        etas = np.ascontiguousarray(etas, np.float32)
+        out = np.zeros(cap, ROOT_DTYPE)
+        stats = np.zeros(7, np.uint64)
+        n = self.f("subdivide_solve", C.c_int64)(
+            C.c_int(K), C.c_uint32(ev), _p(np.asarray(p_beg, np.float32)), _p(np.ascontiguousarray(p_end, np.float32)),
+            _p(tuples), C.c_uint32(len(tuples)), _p(etas), C.c_int(len(etas)), C.c_int(max_depth), C.c_float(eps),
+            C.c_int(max_iterations), C.c_float(cost_tolerance), C.c_int(warm_up),
+            _p(np.ascontiguousarray(tris, np.float32)), _p(np.ascontiguousarray(attribs)), _p(bvh["nodes"]),
+            _p(np.ascontiguousarray(scene_tris, np.float32)), C.c_uint32(bvh["root"]), _p(out), C.c_int64(cap),
+            _p(stats))
+        if n < 0:
+            raise RuntimeError("root capacity exceeded")
+        return out[:n].copy(), stats
+
+    def directed(self, op: int, up: bool, a: float, b: float = 0.0) -> float:
+        """One directed-rounding operation of the subdivision oracle (0 add, 1 sub, 2 mul,
+        3 div downward, 4 sqrt)."""
+        return float(self.f("directed", C.c_float)(C.c_int(op), C.c_int(1 if up else 0), C.c_float(a), C.c_float(b)))
+
+    def subdivide_contribute(self, K, ev, scene, tuples, roots, first_diffuse, etas, tris, attribs, iteration=0):
+        """Binned spectral image (pixels x bins) of subdivision roots; rows' query = pixel."""
+        etas = np.ascontiguousarray(etas, np.float32)
+        fd = np.ascontiguousarray(first_diffuse, np.float32)
+        spectral = np.zeros((fd.shape[0], etas.size), np.float32)
+        self.f("subdivide_contribute")(
+            C.c_int(K), C.c_uint32(ev), _p(_light(scene, iteration)), C.c_float(scene.light_intensity),
+            C.c_float(scene.radiance_clamp), _p(np.ascontiguousarray(tuples, np.uint32)),
+            _p(np.ascontiguousarray(roots)), C.c_int64(len(roots)), _p(fd), _p(etas), C.c_int(etas.size),
+            _p(np.ascontiguousarray(tris, np.float32)), _p(np.ascontiguousarray(attribs)), _p(spectral))
+        return spectral
 
 
 _cache: dict = {}

@@ -2,10 +2,13 @@
 // CPU restatement in pz_oracle.hpp, loaded by tests/ (ctypes) and by bench.py's
 // CPU-baseline leg.  Nothing in the product links or loads this library.
 #include "pz_oracle.hpp"
+#include "pz_oracle_subdiv.hpp"
 
 #include <omp.h>
 
+#include <array>
 #include <atomic>
+#include <tuple>
 #include <cstdio>
 
 using namespace pzo;
@@ -588,6 +591,91 @@ int64_t pzo_path_cuts(int K, uint32_t events, float eta, const float* p_beg, con
         default: return 0;
     }
     return n > cap ? -n : n;
+}
+
+// Subdivision solve (pz_oracle_subdiv.hpp): roots of every tuple row {q, tri[0..K)},
+// sorted by (tuple, bin, depth, path).  The rows index tris / attribs; visibility runs
+// through nodes over scene_tris.  stats[7]: boxes tested, culled, leaves, solves,
+// converged, outside their box, roots.  Returns the root count (negative on overflow).
+int64_t pzo_subdivide_solve(int K, uint32_t events, const float* p_beg, const float* p_end, const uint32_t* tuples,
+                            uint32_t n_tuples, const float* etas, int n_bins, int max_depth, float eps,
+                            int max_iterations, float cost_tolerance, int warm_up, const Triangle* tris,
+                            const TriangleAttrib* attribs, const InternalNode* nodes, const Triangle* scene_tris,
+                            uint32_t root, void* out, int64_t cap, uint64_t* stats)
+{
+    subdiv::Params P{max_depth, eps, max_iterations, cost_tolerance, warm_up};
+    const F3 a = ld3(p_beg);
+    const F3* ends = reinterpret_cast<const F3*>(p_end);
+    std::vector<std::vector<subdiv::Root>> rows(n_tuples);
+    std::vector<std::array<uint64_t, 7>> st(n_tuples);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t r = 0; r < (int64_t)n_tuples; r++) {
+        st[r].fill(0);
+        const uint32_t ri = (uint32_t)r;
+        switch (K) {
+            case 1: subdiv::solve_row<1>(ri, tuples, events, a, ends, etas, n_bins, P, tris, attribs, nodes, scene_tris, root, rows[r], st[r].data()); break;
+            case 2: subdiv::solve_row<2>(ri, tuples, events, a, ends, etas, n_bins, P, tris, attribs, nodes, scene_tris, root, rows[r], st[r].data()); break;
+            case 3: subdiv::solve_row<3>(ri, tuples, events, a, ends, etas, n_bins, P, tris, attribs, nodes, scene_tris, root, rows[r], st[r].data()); break;
+            case 4: subdiv::solve_row<4>(ri, tuples, events, a, ends, etas, n_bins, P, tris, attribs, nodes, scene_tris, root, rows[r], st[r].data()); break;
+            default: break;
+        }
+    }
+    int64_t n = 0;
+    subdiv::Root* o = static_cast<subdiv::Root*>(out);
+    for (int j = 0; j < 7; j++) stats[j] = 0;
+    for (uint32_t r = 0; r < n_tuples; r++) {
+        for (int j = 0; j < 7; j++) stats[j] += st[r][j];
+        auto& v = rows[r];
+        std::sort(v.begin(), v.end(), [](const subdiv::Root& x, const subdiv::Root& y) {
+            return std::make_tuple(x.bin, x.depth, x.path) < std::make_tuple(y.bin, y.depth, y.path);
+        });
+        for (const auto& x : v) {
+            if (n < cap) o[n] = x;
+            n++;
+        }
+    }
+    return n > cap ? -n : n;
+}
+
+// Contributions of subdivision roots to a binned spectral image (the tail of
+// solveSpecularPath<K>, main_gpu.cu:466-486, at each root's bin): rows' query = pixel of
+// first_diffuse (10 floats per pixel).  Accumulates in root order.
+void pzo_subdivide_contribute(int K, uint32_t events, const float* p_beg, float light_intensity, float radiance_clamp,
+                              const uint32_t* tuples, const void* roots, int64_t n_roots, const float* first_diffuse,
+                              const float* etas, int n_bins, const Triangle* tris, const TriangleAttrib* attribs,
+                              float* spectral)
+{
+    const subdiv::Root* rs = static_cast<const subdiv::Root*>(roots);
+    const F3 L = ld3(p_beg);
+    for (int64_t i = 0; i < n_roots; i++) {
+        const subdiv::Root& r = rs[i];
+        const uint32_t* t = tuples + (size_t)r.tuple * (1 + K);
+        const uint32_t px = t[0];
+        Triangle tk[4];
+        TriangleAttrib ak[4];
+        for (int k = 0; k < K; k++) { tk[k] = tris[t[1 + k]]; ak[k] = attribs[t[1 + k]]; }
+        const float* fd = first_diffuse + 10 * (size_t)px;
+        const F3 p = mk(fd[0], fd[1], fd[2]), n = mk(fd[3], fd[4], fd[5]);
+        const float eta = etas[r.bin];
+        const float dadw = dAdw<float>(L, get_vertex<float>(0, tk, r.params) - L, p, tk, ak, events, eta);
+        const float cosv = std::fmax(dot(normalize(get_vertex<float>(K - 1, tk, r.params) - p), n), 0.0f);
+        float c = r.throughput * light_intensity / dadw * cosv;
+        c = std::fmin(c, radiance_clamp);
+        spectral[(size_t)px * n_bins + r.bin] += c;
+    }
+}
+
+// One directed-rounding operation of the subdivision oracle (op 0 add, 1 sub, 2 mul,
+// 3 div (downward only), 4 sqrt; up = 1 rounds toward +inf, 0 toward -inf).
+float pzo_directed(int op, int up, float a, float b)
+{
+    switch (op) {
+        case 0: return up ? subdiv::add_u(a, b) : subdiv::add_d(a, b);
+        case 1: return up ? subdiv::sub_u(a, b) : subdiv::sub_d(a, b);
+        case 2: return up ? subdiv::mul_u(a, b) : subdiv::mul_d(a, b);
+        case 3: return subdiv::div_d(a, b);
+        default: return up ? subdiv::sqrt_u(a) : subdiv::sqrt_d(a);
+    }
 }
 
 }  // extern "C"

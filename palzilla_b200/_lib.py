@@ -38,6 +38,16 @@ class BatchTuning(C.Structure):
     _fields_ = [("p1_blocks_per_sm", C.c_int), ("p2_blocks_per_sm", C.c_int), ("p2_chunk", C.c_int)]
 
 
+class SubdivParams(C.Structure):
+    _fields_ = [("max_depth", C.c_int), ("eps", C.c_float), ("max_iterations", C.c_int),
+                ("cost_tolerance", C.c_float), ("early_term_warmup", C.c_int), ("fp64_polish", C.c_int)]
+
+
+class SubdivStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("boxes_tested", "boxes_culled", "leaves", "solves", "converged",
+                                          "outside_box", "roots", "polished")]
+
+
 class SolveDesc(C.Structure):
     _fields_ = [("K", i32), ("events", u32), ("paths", vp), ("n_paths", u64), ("first_diffuse", vp),
                 ("internals", vp), ("root", vp), ("triangles", vp), ("attribs", vp), ("cache", vp),
@@ -86,6 +96,10 @@ SIGNATURES = {
     "pz_path_cuts_scratch_bytes": (sz, [i32, u32]),
     "pz_path_cuts": (i32, [i32, u32, f32, Float3, vp, u32, vp, vp, vp, vp, vp, i32, vp, u32, C.POINTER(u64),
                            C.POINTER(u64), vp, sz, vp]),
+    "pz_subdivide_scratch_bytes": (sz, [u64]),
+    "pz_subdivide_solve": (i32, [i32, u32, Float3, vp, vp, u32, vp, i32, C.POINTER(SubdivParams), vp, vp, vp, vp, vp,
+                                 vp, u64, C.POINTER(u64), C.POINTER(SubdivStats), vp, sz, vp]),
+    "pz_subdivide_contribute": (i32, [i32, u32, Float3, f32, f32, vp, vp, u64, vp, vp, i32, vp, vp, vp, vp]),
     "pz_adjoint_forward": (i32, [C.POINTER(SolveDesc), vp]),
     "pz_adjoint_backward": (i32, [C.POINTER(SolveDesc), vp, vp, vp, vp, vp]),
     "pz_resolve": (i32, [vp, vp, i32, vp]),

@@ -191,13 +191,15 @@ class PathCache:
 
 def photon_trace(ds: DeviceScene, cache: PathCache | None, iteration: int = 0, photons_per_triangle=None,
                  eta_range=None, records: bool = False, stream=None):
-    """photonTrace (main_gpu.cu:56-211).  Returns the per-photon record tensor when asked."""
+    """photonTrace (main_gpu.cu:56-211) from the light point of this iteration
+    (Scene.light_point).  Returns the per-photon record tensor when asked."""
     sc = ds.scene
     ppt = photons_per_triangle or sc.photons_per_triangle
     emin, emax = eta_range or sc.eta_range()
     rec = torch.empty(ds.n * ppt * 64, dtype=torch.uint8, device=ds.tris.device) if records else None
     _lib.call("pz_photon_trace", _vp(ds.internals), _vp(ds.root_dev), _vp(ds.tris), _vp(ds.attribs),
-              C.c_int(ds.n), C.c_int(ppt), _lib.f3(sc.p_light), C.c_float(emin), C.c_float(emax), C.c_int(iteration),
+              C.c_int(ds.n), C.c_int(ppt), _lib.f3(sc.light_point(iteration)), C.c_float(emin), C.c_float(emax),
+              C.c_int(iteration),
               C.c_float(sc.min_throughput), _vp(cache.buf if cache else None),
               C.c_uint32(cache.capacity if cache else 0), C.c_float(cache.step if cache else 0.0), _vp(rec),
               C.c_void_p(_stream(stream)))
@@ -235,7 +237,8 @@ def solve_primary(ds: DeviceScene, frame: Frame, iteration: int = 0, lens=(0.6, 
     g = ray_generator(sc)
     l = _lib.LensParams(*[float(x) for x in lens])
     _lib.call("pz_solve_primary", _vp(frame.accum), _vp(frame.fd), C.c_int(sc.width), C.c_int(sc.height), C.byref(g),
-              C.byref(l), _vp(ds.internals), _vp(ds.root_dev), _vp(ds.tris), _vp(ds.attribs), _lib.f3(sc.p_light),
+              C.byref(l), _vp(ds.internals), _vp(ds.root_dev), _vp(ds.tris), _vp(ds.attribs),
+              _lib.f3(sc.light_point(iteration)),
               C.c_float(sc.light_intensity), C.c_float(sc.radiance_clamp), C.c_float(sc.cauchy_a),
               C.c_float(sc.cauchy_b), _lib.f3(sc.albedo), C.c_int(iteration), _vp(frame.status),
               C.c_void_p(_stream(stream)))
@@ -262,7 +265,9 @@ def sort_and_reorder(frame: Frame, n_paths: int, sorter: OnesweepSort, stream=No
 
 def solve_desc(ds: DeviceScene, frame: Frame, cache: PathCache, events_str: str, n_paths: int, spectral=None,
                etas=None, stats=None, max_iterations=32, cost_tolerance=1e-10, early_term_warmup=1, exact=False,
-               polish_det=0.0, continuation=False, fold_det=0.0):
+               polish_det=0.0, continuation=False, fold_det=0.0, iteration=0):
+    """Solve descriptor of one event string; the light is the point of this iteration
+    (Scene.light_point)."""
     from .scenes import event_descriptor
     sc = ds.scene
     d = _lib.SolveDesc()
@@ -278,7 +283,7 @@ def solve_desc(ds: DeviceScene, frame: Frame, cache: PathCache, events_str: str,
     d.cache = cache.buf.data_ptr()
     d.cache_capacity = cache.capacity
     d.cell_step = cache.step
-    d.p_light = _lib.f3(sc.p_light)
+    d.p_light = _lib.f3(sc.light_point(iteration))
     d.light_intensity = sc.light_intensity
     d.radiance_clamp = sc.radiance_clamp
     d.cauchy_a = sc.cauchy_a
@@ -367,6 +372,77 @@ class PathCuts:
                   _vp(builder.m_rootNode), C.c_int(1 if directed else 0), _vp(out), C.c_uint32(self.tuple_capacity),
                   C.byref(nt), C.byref(visited), _vp(buf), C.c_size_t(buf.numel()), C.c_void_p(_stream(stream)))
         return out[: nt.value], visited.value
+
+
+# ---------------------------------------------------------------------------------------
+# subdivision solve
+# ---------------------------------------------------------------------------------------
+ROOT_FIELDS = ("tuple", "bin", "depth", "path")
+
+
+class SubdivisionSolver:
+    """Per-tuple parametric-domain subdivision under affine bounds, then Newton in the
+    surviving boxes (pz_subdivide_solve; no reference counterpart).
+
+    ``run(K, events, p_beg, p_end, tuples, etas, triangles, attribs, scene_builder,
+    scene_triangles)``: ``tuples`` is an int32 (n, 1 + K) tensor of {query, triangle[K]}
+    rows indexing ``triangles`` / ``attribs`` (what PathCuts.run or work_list_rows
+    return); visibility runs through the scene's BVH.  Returns (ids, params, throughput,
+    stats): ids an int64 (m, 4) tensor of {tuple row, bin, depth, path} per root, params
+    float (m, 2K), throughput float (m,), stats a dict of the kernel's counters."""
+
+    def __init__(self, device="cuda", box_capacity: int = 1 << 22, root_capacity: int = 1 << 20, max_depth: int = 12,
+                 eps: float = 1e-4, max_iterations: int = 32, cost_tolerance: float = 1e-10,
+                 early_term_warmup: int = 1, fp64_polish: bool = False):
+        self.device = device
+        self.box_capacity = box_capacity
+        self.root_capacity = root_capacity
+        self.params = _lib.SubdivParams(max_depth, eps, max_iterations, cost_tolerance, early_term_warmup,
+                                        1 if fp64_polish else 0)
+        self.scratch = Scratch(device)
+        self.roots = torch.empty(root_capacity * 64, dtype=torch.uint8, device=device)
+
+    def run(self, K: int, events: int, p_beg, p_end, tuples, etas, triangles, attribs, scene_builder: BVHGPUBuilder,
+            scene_triangles, stream=None):
+        n = int(tuples.shape[0])
+        cap = max(self.box_capacity, n)
+        buf = self.scratch.get(_lib.lib().pz_subdivide_scratch_bytes(cap))
+        nr = C.c_uint64(0)
+        st = _lib.SubdivStats()
+        _lib.call("pz_subdivide_solve", C.c_int(K), C.c_uint32(events), _lib.f3(p_beg), _vp(p_end), _vp(tuples),
+                  C.c_uint32(n), _vp(etas), C.c_int(int(etas.numel())), C.byref(self.params), _vp(triangles),
+                  _vp(attribs), _vp(scene_builder.m_internals), _vp(scene_triangles), _vp(scene_builder.m_rootNode),
+                  _vp(self.roots), C.c_uint64(self.root_capacity), C.byref(nr), C.byref(st), _vp(buf),
+                  C.c_size_t(buf.numel()), C.c_void_p(_stream(stream)))
+        m = nr.value
+        rec = self.roots[: m * 64].view(torch.int32).view(m, 16)
+        ids = rec[:, :4].to(torch.int64) & 0xFFFFFFFF
+        params = rec[:, 4:4 + 2 * K].contiguous().view(torch.float32)
+        thr = rec[:, 12].contiguous().view(torch.float32)
+        stats = {f: int(getattr(st, f)) for f, _ in _lib.SubdivStats._fields_}
+        return ids, params, thr, stats
+
+    def contribute(self, K: int, events: int, scene, tuples, n_roots: int, frame: "Frame", etas, triangles, attribs,
+                   spectral, iteration: int = 0, stream=None):
+        """Adds the roots of the last run() to `spectral` (pixels x bins); the tuple rows'
+        query index is the pixel of frame's FirstDiffuse records (pz_subdivide_contribute)."""
+        _lib.call("pz_subdivide_contribute", C.c_int(K), C.c_uint32(events), _lib.f3(scene.light_point(iteration)),
+                  C.c_float(scene.light_intensity), C.c_float(scene.radiance_clamp), _vp(tuples), _vp(self.roots),
+                  C.c_uint64(n_roots), _vp(frame.fd), _vp(etas), C.c_int(int(etas.numel())), _vp(triangles),
+                  _vp(attribs), _vp(spectral), C.c_void_p(_stream(stream)))
+
+
+def receiver_points(frame: "Frame"):
+    """The receiver point of every pixel (FirstDiffuse.p), a contiguous float (npx, 3)."""
+    return frame.fd.view(torch.float32).view(frame.npx, 10)[:, :3].contiguous()
+
+
+def work_list_rows(frame: "Frame", cache: PathCache, n_paths: int, K: int):
+    """{pixel, triangle[K]} rows (int32, n_paths x (1 + K)) of a frame's work list -- one
+    per (pixel, cached tuple) -- the rows pz_subdivide_solve takes."""
+    sp = frame.paths[: n_paths * 8].view(torch.int32).view(n_paths, 2)
+    tris = cache.views()["tris"].view(-1, 4)
+    return torch.cat([sp[:, :1], tris[sp[:, 1].long(), :K]], 1).contiguous()
 
 
 # ---------------------------------------------------------------------------------------

@@ -3,8 +3,8 @@ C++ facade's driver program palzilla_b200/pk_render.
 
 Each translation unit is compiled with nvcc for sm_100a.  Units whose results must
 be bit-exact with the CPU oracle (BVH keys, traversal, photons, eye pass, the batched
-solver, path cuts, the adjoint) are built with -fmad=false so that no multiply-add pair
-is contracted into an FMA; the plain solver is built both ways.  Objects are rebuilt
+solver, path cuts, the adjoint, the subdivision solve) are built with -fmad=false so
+that no multiply-add pair is contracted into an FMA; the plain solver is built both ways.  Objects are rebuilt
 only when a source or header is newer than the object.
 """
 from __future__ import annotations
@@ -42,6 +42,7 @@ UNITS = {
     "pz_sort_static": ("pz_sort_static.cu", []),
     "pz_pathcuts": ("pz_pathcuts.cu", ["-fmad=false"]),
     "pz_adjoint": ("pz_adjoint.cu", ["-fmad=false"]),
+    "pz_subdiv": ("pz_subdiv.cu", ["-fmad=false"]),
 }
 
 

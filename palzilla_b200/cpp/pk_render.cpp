@@ -5,8 +5,9 @@
 //   pk_render scene.bin out.bin
 //
 // scene.bin (little endian): int32 n, width, height, iterations; float eye[3], center[3],
-// up[3], fovy, p_light[3], light_intensity, radiance_clamp, min_throughput, cauchy_a,
-// cauchy_b; pz_triangle[n]; pz_triangle_attrib[n].
+// up[3], fovy, p_light[3], light_size[2] (area light extent along x and z; 0 0 = point
+// light), light_intensity, radiance_clamp, min_throughput, cauchy_a, cauchy_b;
+// pz_triangle[n]; pz_triangle_attrib[n].
 // out.bin: float accum[width * height * 4]; uint32 pixels[width * height]; uint64 paths.
 #include <cstdio>
 #include <vector>
@@ -22,7 +23,7 @@ int main(int argc, char** argv)
     std::FILE* f = std::fopen(argv[1], "rb");
     if (!f) return 2;
     int32_t hdr[4];
-    float cam[10], light[3], params[5];
+    float cam[10], light[5], params[5];
     bool ok = std::fread(hdr, sizeof(hdr), 1, f) == 1 && std::fread(cam, sizeof(cam), 1, f) == 1 &&
               std::fread(light, sizeof(light), 1, f) == 1 && std::fread(params, sizeof(params), 1, f) == 1;
     const int n = hdr[0], width = hdr[1], height = hdr[2], iterations = hdr[3];
@@ -41,6 +42,8 @@ int main(int argc, char** argv)
         r.m_camera.lookat({cam[0], cam[1], cam[2]}, {cam[3], cam[4], cam[5]}, {cam[6], cam[7], cam[8]}, cam[9], width,
                           height);
         r.m_p_light = {light[0], light[1], light[2]};
+        r.m_lightSize[0] = light[3];
+        r.m_lightSize[1] = light[4];
         r.m_lightIntencity = params[0];
         r.m_radianceClamp = params[1];
         r.m_minThroughput = params[2];

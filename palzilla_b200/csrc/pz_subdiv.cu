@@ -1,0 +1,762 @@
+// pz_subdiv.cu -- per-tuple parametric-domain subdivision under affine bounds, and the
+// Newton solve in the boxes that survive.
+//
+// No reference counterpart.  The reference solves each admissible tuple once, from one
+// start (main.cpp:1052, solveConstraints<K>, pk.h:466-592), and so finds at most one root
+// per tuple.  Here the domain of every tuple -- its 2K barycentrics, the unit box
+// [0,1]^2K -- is bisected level by level: split t halves dimension t mod 2K, so a box is
+// named by its depth and the bits of its bisection path.  A box is dropped when
+//   - it lies outside a triangle (u_lo + v_lo > 1 for some vertex), or
+//   - an affine bound of the specular constraint the Newton solver drives to zero
+//     (the cross product of the outgoing direction with the reflected / refracted one,
+//     taken on the side of the shading normal the solver takes) excludes zero in some
+//     component: no root lies in the box, or
+//   - the sign pattern of the two cosines at some vertex rules out the event over the
+//     whole box, which contributableThroughput (pk.h:760-842) would reject.
+// A box stops splitting at the depth limit, or when every bounded residual component is
+// narrower than eps (the bound no longer tightens usefully).  Its centre then starts the
+// reference's Newton solve, once per wavelength bin.  A root is kept when
+//   - the solve converged,
+//   - the root lies in that box (half-open boxes: every root has one owner box, so no
+//     root is reported twice),
+//   - contributableThroughput, visibility included, is positive.
+// The wavelength bins share one subdivision: the bound takes eta^2 - 1 over the range of
+// the bins' values, so a box that survives for any bin survives.
+//
+// Affine forms: x = c + sum_i x_i e_i + r e_err with |e_i|, |e_err| <= 1; the noise
+// symbols e_i are the box's 2K parameters.  Central and linear coefficients are rounded
+// to nearest; each rounding error, and each nonlinear remainder, goes into the radius r
+// with upward rounding, so the bound encloses the constraint in exact arithmetic.  The
+// unit is built with -fmad=false, so the CPU oracle can repeat every operation.
+//
+// Kernels: k_sub_init (one entry per tuple), k_sub_round (one launch per depth; a thread
+// per box: bound, cull, split or retire to the leaf list; warp-aggregated appends),
+// k_sub_leaves (a thread per (leaf, bin): Newton, ownership, throughput, root output),
+// k_sub_contribute (a thread per root: dAdw and the binned spectral image).  The rounds
+// read their input count on the device: no host synchronisation between launches.
+#include <algorithm>
+
+#include "pz_capi_internal.h"
+#include "pz_common.cuh"
+#include "pz_frame.cuh"
+#include "pz_solver.cuh"
+
+namespace pz {
+namespace subdiv {
+
+using solver::Chain;
+using solver::V3;
+
+constexpr int kBlock = 256;
+constexpr int kMaxDepth = 20;  // path bits in an entry
+constexpr int kMaxBins = 256;
+constexpr uint32_t kPathMask = (1u << kMaxDepth) - 1u;
+
+enum : int { kStTested = 0, kStCulled, kStSolves, kStConverged, kStOutside, kStRoots, kStPolished, kNumStats };
+
+// ---------------------------------------------------------------- affine forms
+// Rounding error of one round-to-nearest result r: at most |r| 2^-24 (normal) or 2^-150.
+PZ_D float rerr(float r) { return __fadd_ru(__fmul_ru(fabsf(r), 0x1p-24f), 0x1p-149f); }
+
+template <int N> struct Af {
+    float c, x[N], r;
+};
+template <int N> struct Af3 {
+    Af<N> x, y, z;
+};
+
+template <int N> PZ_D Af<N> af_const(float v)
+{
+    Af<N> o;
+    o.c = v;
+#pragma unroll
+    for (int i = 0; i < N; i++) o.x[i] = 0.0f;
+    o.r = 0.0f;
+    return o;
+}
+
+template <int N> PZ_D Af<N> af_add(const Af<N>& a, const Af<N>& b)
+{
+    Af<N> o;
+    o.c = __fadd_rn(a.c, b.c);
+    float r = __fadd_ru(__fadd_ru(a.r, b.r), rerr(o.c));
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        o.x[i] = __fadd_rn(a.x[i], b.x[i]);
+        r = __fadd_ru(r, rerr(o.x[i]));
+    }
+    o.r = r;
+    return o;
+}
+
+template <int N> PZ_D Af<N> af_sub(const Af<N>& a, const Af<N>& b)
+{
+    Af<N> o;
+    o.c = __fsub_rn(a.c, b.c);
+    float r = __fadd_ru(__fadd_ru(a.r, b.r), rerr(o.c));
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        o.x[i] = __fsub_rn(a.x[i], b.x[i]);
+        r = __fadd_ru(r, rerr(o.x[i]));
+    }
+    o.r = r;
+    return o;
+}
+
+template <int N> PZ_D Af<N> af_neg(const Af<N>& a)
+{
+    Af<N> o;
+    o.c = -a.c;
+#pragma unroll
+    for (int i = 0; i < N; i++) o.x[i] = -a.x[i];
+    o.r = a.r;
+    return o;
+}
+
+// sum |x_i| + r, rounded up
+template <int N> PZ_D float af_rad(const Af<N>& a)
+{
+    float s = a.r;
+#pragma unroll
+    for (int i = 0; i < N; i++) s = __fadd_ru(s, fabsf(a.x[i]));
+    return s;
+}
+template <int N> PZ_D float af_lo(const Af<N>& a) { return __fsub_rd(a.c, af_rad(a)); }
+template <int N> PZ_D float af_hi(const Af<N>& a) { return __fadd_ru(a.c, af_rad(a)); }
+
+// a*b = ac bc + ac (Lb + Eb) + bc (La + Ea) + (La + Ea)(Lb + Eb); the linear parts are
+// kept, the rest is bounded by |ac| rb_err + |bc| ra_err + rad(a) rad(b).
+template <int N> PZ_D Af<N> af_mul(const Af<N>& a, const Af<N>& b)
+{
+    Af<N> o;
+    o.c = __fmul_rn(a.c, b.c);
+    float r = rerr(o.c);
+    float ra = a.r, rb = b.r;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        const float p = __fmul_rn(a.c, b.x[i]), q = __fmul_rn(b.c, a.x[i]);
+        o.x[i] = __fadd_rn(p, q);
+        r = __fadd_ru(r, __fadd_ru(__fadd_ru(rerr(p), rerr(q)), rerr(o.x[i])));
+        ra = __fadd_ru(ra, fabsf(a.x[i]));
+        rb = __fadd_ru(rb, fabsf(b.x[i]));
+    }
+    r = __fadd_ru(r, __fmul_ru(fabsf(a.c), b.r));
+    r = __fadd_ru(r, __fmul_ru(fabsf(b.c), a.r));
+    o.r = __fadd_ru(r, __fmul_ru(ra, rb));
+    return o;
+}
+
+// a * s for an exact float s
+template <int N> PZ_D Af<N> af_scale(const Af<N>& a, float s)
+{
+    Af<N> o;
+    o.c = __fmul_rn(a.c, s);
+    float r = __fadd_ru(__fmul_ru(a.r, fabsf(s)), rerr(o.c));
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        o.x[i] = __fmul_rn(a.x[i], s);
+        r = __fadd_ru(r, rerr(o.x[i]));
+    }
+    o.r = r;
+    return o;
+}
+
+// a + s for an exact float s
+template <int N> PZ_D Af<N> af_addc(const Af<N>& a, float s)
+{
+    Af<N> o = a;
+    o.c = __fadd_rn(a.c, s);
+    o.r = __fadd_ru(a.r, rerr(o.c));
+    return o;
+}
+
+// sqrt on [lo, hi], lo >= 0, by the min-range linearisation sqrt(x) = alpha x + d(x),
+// alpha <= 1 / (2 sqrt(hi)) so that d is nondecreasing on [lo, hi] and lies in
+// [d(lo), d(hi)] = zeta -+ delta.
+template <int N> PZ_D Af<N> af_sqrt(const Af<N>& a)
+{
+    const float lo = fmaxf(af_lo(a), 0.0f), hi = af_hi(a);
+    if (!(hi > 0.0f)) return af_const<N>(0.0f);
+    const float sh = __fsqrt_ru(hi);
+    const float alpha = __fdiv_rd(1.0f, __fmul_ru(2.0f, sh));
+    const float dlo = __fsub_rd(__fsqrt_rd(lo), __fmul_ru(alpha, lo));
+    const float dhi = __fsub_ru(sh, __fmul_rd(alpha, hi));
+    const float zeta = __fmul_rn(__fadd_rn(dlo, dhi), 0.5f);
+    const float delta = fmaxf(__fsub_ru(dhi, zeta), __fsub_ru(zeta, dlo));
+    Af<N> o = af_addc(af_scale(a, alpha), zeta);
+    o.r = __fadd_ru(o.r, delta);
+    return o;
+}
+
+template <int N> PZ_D Af3<N> af3_const(float3 v) { return Af3<N>{af_const<N>(v.x), af_const<N>(v.y), af_const<N>(v.z)}; }
+template <int N> PZ_D Af3<N> af3_sub(const Af3<N>& a, const Af3<N>& b)
+{
+    return Af3<N>{af_sub(a.x, b.x), af_sub(a.y, b.y), af_sub(a.z, b.z)};
+}
+template <int N> PZ_D Af3<N> af3_add(const Af3<N>& a, const Af3<N>& b)
+{
+    return Af3<N>{af_add(a.x, b.x), af_add(a.y, b.y), af_add(a.z, b.z)};
+}
+template <int N> PZ_D Af3<N> af3_mul(const Af3<N>& a, const Af<N>& s)
+{
+    return Af3<N>{af_mul(a.x, s), af_mul(a.y, s), af_mul(a.z, s)};
+}
+template <int N> PZ_D Af<N> af3_dot(const Af3<N>& a, const Af3<N>& b)
+{
+    return af_add(af_add(af_mul(a.x, b.x), af_mul(a.y, b.y)), af_mul(a.z, b.z));
+}
+template <int N> PZ_D Af3<N> af3_cross(const Af3<N>& a, const Af3<N>& b)
+{
+    return Af3<N>{af_sub(af_mul(a.y, b.z), af_mul(a.z, b.y)), af_sub(af_mul(a.z, b.x), af_mul(a.x, b.z)),
+                  af_sub(af_mul(a.x, b.y), af_mul(a.y, b.x))};
+}
+// p0 + e0 u + e1 v (the Newton solver's vertex and shading-normal interpolation)
+template <int N> PZ_D Af<N> af_lin(float p0, float e0, float e1, const Af<N>& u, const Af<N>& v)
+{
+    return af_add(af_addc(af_scale(u, e0), p0), af_scale(v, e1));
+}
+template <int N> PZ_D Af3<N> af3_lin(float3 p0, float3 e0, float3 e1, const Af<N>& u, const Af<N>& v)
+{
+    return Af3<N>{af_lin(p0.x, e0.x, e1.x, u, v), af_lin(p0.y, e0.y, e1.y, u, v), af_lin(p0.z, e0.z, e1.z, u, v)};
+}
+
+// ---------------------------------------------------------------- boxes
+// Box of depth d with bisection path `path`: dimension j is halved at splits j, j + N,
+// j + 2N, ... < d; bit t of the path is the half taken at split t.
+template <int N> PZ_D void box_bounds(uint32_t path, int depth, float* lo, float* hi)
+{
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+        float l = 0.0f, w = 1.0f;
+        for (int t = j; t < depth; t += N) {
+            w *= 0.5f;
+            if ((path >> t) & 1u) l += w;
+        }
+        lo[j] = l;
+        hi[j] = l + w;
+    }
+}
+
+enum Verdict : int { kCull = 0, kSplit = 1, kLeaf = 2 };
+
+// The bound of one box.  em1: eta^2 - 1 over the bins, as an affine constant.
+template <int K>
+PZ_D int bound_box(const Chain<K>& ch, float3 pBeg, float3 pEnd, uint32_t events, const Af<2 * K>& em1,
+                   const float* lo, const float* hi, float eps)
+{
+    constexpr int N = 2 * K;
+#pragma unroll
+    for (int k = 0; k < K; k++)
+        if (__fadd_rd(lo[2 * k], lo[2 * k + 1]) > 1.0f) return kCull;  // outside the triangle
+    Af3<N> X[K + 2], Nrm[K];
+    X[0] = af3_const<N>(pBeg);
+    X[K + 1] = af3_const<N>(pEnd);
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        Af<N> u = af_const<N>(__fmul_rn(__fadd_rn(lo[2 * k], hi[2 * k]), 0.5f));
+        Af<N> v = af_const<N>(__fmul_rn(__fadd_rn(lo[2 * k + 1], hi[2 * k + 1]), 0.5f));
+        u.x[2 * k] = __fmul_rn(__fsub_rn(hi[2 * k], lo[2 * k]), 0.5f);
+        v.x[2 * k + 1] = __fmul_rn(__fsub_rn(hi[2 * k + 1], lo[2 * k + 1]), 0.5f);
+        X[k + 1] = af3_lin(ch.v0[k], ch.e0[k], ch.e1[k], u, v);
+        Nrm[k] = af3_lin(ch.n0[k], ch.ne0[k], ch.ne1[k], u, v);
+    }
+    bool resolved = true;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        Af3<N> wi = af3_sub(X[k], X[k + 1]);
+        Af3<N> wo = af3_sub(X[k + 2], X[k + 1]);
+        const Af3<N>& n = Nrm[k];
+        const Af<N> s = af3_dot(wi, n), t = af3_dot(wo, n);
+        const float sl = af_lo(s), sh = af_hi(s), tl = af_lo(t), th = af_hi(t);
+        const bool refract = (events >> k) & 1u;
+        // the event needs (wi.n)(wo.n) <= 0 (T) or > 0 (R) somewhere in the box
+        if (refract ? ((sl > 0.0f && tl > 0.0f) || (sh < 0.0f && th < 0.0f))
+                    : ((sl >= 0.0f && th <= 0.0f) || (sh <= 0.0f && tl >= 0.0f)))
+            return kCull;
+        // the solver refracts / reflects the direction on the normal's side of the surface
+        if (sh < 0.0f) {
+            const Af3<N> tmp = wi;
+            wi = wo;
+            wo = tmp;
+        } else if (!(sl >= 0.0f)) {
+            resolved = false;  // the side changes inside the box: no bound at this vertex
+            continue;
+        }
+        const Af<N> NoN = af3_dot(n, n);
+        const Af<N> WIoN = af3_dot(wi, n);
+        Af3<N> w;
+        if (refract) {
+            // -wi (n.n) + n ((wi.n) - sqrt((n.n)(wi.wi)(eta^2 - 1) + (wi.n)^2)), pk.h:181-200
+            const Af<N> WoW = af3_dot(wi, wi);
+            const Af<N> kk = af_add(af_mul(af_mul(NoN, WoW), em1), af_mul(WIoN, WIoN));
+            if (!(af_lo(kk) >= 0.0f)) {  // total internal reflection in part of the box
+                resolved = false;
+                continue;
+            }
+            const Af<N> g = af_sub(WIoN, af_sqrt(kk));
+            w = af3_add(Af3<N>{af_neg(af_mul(wi.x, NoN)), af_neg(af_mul(wi.y, NoN)), af_neg(af_mul(wi.z, NoN))},
+                        af3_mul(n, g));
+        } else {
+            // (n.n) times the reflection n (wi.n) 2 / (n.n) - wi: the same zeros for n != 0
+            if (!(af_lo(NoN) > 0.0f)) {
+                resolved = false;
+                continue;
+            }
+            const Af<N> d2 = af_scale(WIoN, 2.0f);
+            w = af3_sub(af3_mul(n, d2), af3_mul(wi, NoN));
+        }
+        const Af3<N> c = af3_cross(wo, w);
+        const Af<N>* cc[3] = {&c.x, &c.y, &c.z};
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const float l = af_lo(*cc[j]), h = af_hi(*cc[j]);
+            if (l > 0.0f || h < 0.0f) return kCull;
+            resolved = resolved && __fsub_ru(h, l) < eps;
+        }
+    }
+    return resolved ? kLeaf : kSplit;
+}
+
+// ---------------------------------------------------------------- kernels
+struct SubArgs {
+    uint32_t events;
+    float3 pBeg;
+    const float3* pEnd;
+    const uint32_t* tuples;  // (1 + K) u32 per row: query, triangles
+    uint32_t nRows;
+    const float* etas;
+    uint32_t nBins;
+    int maxDepth;
+    float eps;
+    int maxIterations;
+    float costTolerance;
+    int warmUp;
+    int polish;
+    const Tri* tris;  // the triangles the tuple rows index
+    const Attrib* attribs;
+    const Node* nodes;  // visibility: the scene's BVH and triangles
+    const Tri* sceneTris;
+    const uint32_t* root;
+    uint64_t capacity;  // entries per frontier and in the leaf list
+    float* em1;         // [2]: range of eta^2 - 1 over the bins
+    uint64_t* leaves;
+    unsigned long long* nLeaves;
+    pz_specular_root* roots;
+    unsigned long long* nRoots;
+    uint64_t rootCapacity;
+    unsigned long long* stats;
+    uint32_t* status;
+};
+
+// entry: row << 32 | depth << 20 | path
+PZ_D uint64_t make_entry(uint32_t row, int depth, uint32_t path)
+{
+    return ((uint64_t)row << 32) | ((uint64_t)depth << kMaxDepth) | (path & kPathMask);
+}
+
+PZ_D unsigned long long warp_append(unsigned long long* counter, bool want)
+{
+    const uint32_t active = __activemask();
+    const uint32_t ballot = __ballot_sync(active, want);
+    const int leader = __ffs(active) - 1;
+    unsigned long long base = 0;
+    if ((int)(threadIdx.x & 31) == leader && ballot) base = atomicAdd(counter, (unsigned long long)__popc(ballot));
+    base = __shfl_sync(active, base, leader);
+    return base + __popc(ballot & ((1u << (threadIdx.x & 31)) - 1u));
+}
+
+PZ_D void warp_count(unsigned long long* stat, bool v)
+{
+    const uint32_t active = __activemask();
+    const uint32_t b = __ballot_sync(active, v);
+    if ((int)(threadIdx.x & 31) == __ffs(active) - 1 && b) atomicAdd(stat, (unsigned long long)__popc(b));
+}
+
+template <int K>
+PZ_D void load_row(Chain<K>& ch, const SubArgs& a, uint32_t row, uint32_t* q)
+{
+    const uint32_t* t = a.tuples + (size_t)row * (1 + K);
+    int idx[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) idx[k] = (int)__ldg(t + 1 + k);
+    *q = __ldg(t);
+    solver::load_chain<K>(ch, a.tris, a.attribs, idx);
+}
+
+// eta^2 - 1 over the bins, the way the solver forms it; then the first frontier
+__global__ void k_sub_init(SubArgs a, uint64_t* front, unsigned long long* count)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        float lo = 0.0f, hi = 0.0f;
+        for (uint32_t b = 0; b < a.nBins; b++) {
+            const float e = a.etas[b];
+            const float m = __fsub_rn(__fmul_rn(e, e), 1.0f);
+            lo = b == 0 ? m : fminf(lo, m);
+            hi = b == 0 ? m : fmaxf(hi, m);
+        }
+        a.em1[0] = lo;
+        a.em1[1] = hi;
+        *count = a.nRows;
+    }
+    const uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row < a.nRows) front[row] = make_entry(row, 0, 0u);
+}
+
+template <int K>
+__global__ void __launch_bounds__(kBlock) k_sub_round(SubArgs a, int depth, const uint64_t* __restrict__ frontIn,
+                                                      const unsigned long long* countIn, uint64_t* __restrict__ frontOut,
+                                                      unsigned long long* countOut)
+{
+    constexpr int N = 2 * K;
+    const uint64_t nIn = min((uint64_t)*countIn, a.capacity);
+    // eta^2 - 1 over the bins: centre and radius, rounded outward
+    const float mLo = a.em1[0], mHi = a.em1[1];
+    Af<N> em1 = af_const<N>(__fmul_rn(__fadd_rn(mLo, mHi), 0.5f));
+    em1.r = fmaxf(__fsub_ru(mHi, em1.c), __fsub_ru(em1.c, mLo));
+    const bool last = depth >= a.maxDepth;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nIn; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t ent = frontIn[e];
+        const uint32_t row = (uint32_t)(ent >> 32), path = (uint32_t)ent & kPathMask;
+        Chain<K> ch;
+        uint32_t q;
+        load_row<K>(ch, a, row, &q);
+        float lo[N], hi[N];
+        box_bounds<N>(path, depth, lo, hi);
+        int v = bound_box<K>(ch, a.pBeg, a.pEnd[q], a.events, em1, lo, hi, a.eps);
+        if (v == kSplit && last) v = kLeaf;
+        if (a.stats) {
+            warp_count(a.stats + kStTested, true);
+            warp_count(a.stats + kStCulled, v == kCull);
+        }
+        const unsigned long long ls = warp_append(a.nLeaves, v == kLeaf);
+        if (v == kLeaf) {
+            if (ls < a.capacity) a.leaves[ls] = make_entry(row, depth, path);
+            else raise_error(a.status, kErrCapacity);
+        }
+        const bool split = v == kSplit;
+        for (uint32_t half = 0; half < 2; half++) {
+            const unsigned long long s = warp_append(countOut, split);
+            if (split) {
+                if (s < a.capacity) frontOut[s] = make_entry(row, depth + 1, path | (half << depth));
+                else raise_error(a.status, kErrCapacity);
+            }
+        }
+    }
+}
+
+// FP64 polish of a float root (4 Newton steps); kept when it converged next to the root.
+template <int K>
+__device__ __noinline__ void polish_root(float* xs, const Chain<K>& ch, float3 pBeg, float3 pEnd, uint32_t events,
+                                         float eta)
+{
+    double xd[2 * K];
+#pragma unroll
+    for (int i = 0; i < 2 * K; i++) xd[i] = xs[i];
+    const bool ok = solver::solve_constraints<double, K>(xd, solver::v3f<double>(pBeg), solver::v3f<double>(pEnd), ch,
+                                                         (double)eta, events, 4, 1.0e-24, 4);
+    double moved = 0.0;
+#pragma unroll
+    for (int i = 0; i < 2 * K; i++) moved = fmax(moved, fabs(xd[i] - (double)xs[i]));
+    if (ok && moved < 1.0e-3) {
+#pragma unroll
+        for (int i = 0; i < 2 * K; i++) xs[i] = (float)xd[i];
+    }
+}
+
+template <int K>
+__global__ void __launch_bounds__(kBlock) k_sub_leaves(SubArgs a)
+{
+    constexpr int N = 2 * K;
+    const uint64_t nItems = min((uint64_t)*a.nLeaves, a.capacity) * a.nBins;
+    const uint32_t root = __ldg(a.root);
+    for (uint64_t it = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; it < nItems;
+         it += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t ent = a.leaves[it / a.nBins];
+        const uint32_t bin = (uint32_t)(it % a.nBins);
+        const uint32_t row = (uint32_t)(ent >> 32), path = (uint32_t)ent & kPathMask;
+        const int depth = (int)(((uint32_t)ent >> kMaxDepth) & 31u);
+        Chain<K> ch;
+        uint32_t q;
+        load_row<K>(ch, a, row, &q);
+        float lo[N], hi[N], xs[N];
+        box_bounds<N>(path, depth, lo, hi);
+#pragma unroll
+        for (int j = 0; j < N; j++) xs[j] = __fmul_rn(__fadd_rn(lo[j], hi[j]), 0.5f);
+        const float eta = a.etas[bin];
+        const float3 pEnd = a.pEnd[q];
+        const bool conv = solver::solve_constraints<float, K>(xs, solver::v3f<float>(a.pBeg), solver::v3f<float>(pEnd),
+                                                              ch, eta, a.events, a.maxIterations, a.costTolerance,
+                                                              a.warmUp);
+        bool inside = conv;
+#pragma unroll
+        for (int j = 0; j < N; j++)
+            inside = inside && lo[j] <= xs[j] && (xs[j] < hi[j] || (hi[j] == 1.0f && xs[j] == 1.0f));
+        if (inside && a.polish) polish_root<K>(xs, ch, a.pBeg, pEnd, a.events, eta);
+        float thr = 0.0f;
+        if (inside)
+            thr = solver::contributable_throughput<float, K>(xs, solver::v3f<float>(a.pBeg), solver::v3f<float>(pEnd),
+                                                             ch, a.events, a.nodes, a.sceneTris, root, eta);
+        const bool emit = thr > 0.0f;
+        if (a.stats) {
+            warp_count(a.stats + kStSolves, true);
+            warp_count(a.stats + kStConverged, conv);
+            warp_count(a.stats + kStOutside, conv && !inside);
+            warp_count(a.stats + kStRoots, emit);
+            warp_count(a.stats + kStPolished, inside && a.polish);
+        }
+        const unsigned long long s = warp_append(a.nRoots, emit);
+        if (emit) {
+            if (s < a.rootCapacity) {
+                pz_specular_root o;
+                o.tuple = row;
+                o.bin = bin;
+                o.depth = (uint32_t)depth;
+                o.path = path;
+#pragma unroll
+                for (int j = 0; j < 8; j++) o.params[j] = j < N ? xs[j] : 0.0f;
+                o.throughput = thr;
+                o.pad[0] = o.pad[1] = o.pad[2] = 0;
+                a.roots[s] = o;
+            } else {
+                raise_error(a.status, kErrCapacity);
+            }
+        }
+    }
+}
+
+// Contribution of every root to the binned spectral image: the tail of the reference's
+// per-path solve (solveSpecularPath<K>, main_gpu.cu:466-486) with the wavelength fixed to
+// the root's bin: throughput * I / dAdw * cos at the receiver, clamped, added to
+// spectral[q][bin].  The rows' query index q is the pixel of first_diffuse.
+struct ContribArgs {
+    uint32_t events;
+    float3 pBeg;
+    float lightIntensity, radianceClamp;
+    const uint32_t* tuples;
+    const pz_specular_root* roots;
+    uint64_t nRoots;
+    const FirstDiffuse* fds;
+    const float* etas;
+    uint32_t nBins;
+    const Tri* tris;
+    const Attrib* attribs;
+    float* spectral;
+};
+
+template <int K>
+__global__ void __launch_bounds__(kBlock) k_sub_contribute(ContribArgs a)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.nRoots;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const pz_specular_root r = a.roots[i];
+        const uint32_t* t = a.tuples + (size_t)r.tuple * (1 + K);
+        const uint32_t px = __ldg(t);
+        int idx[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) idx[k] = (int)__ldg(t + 1 + k);
+        Chain<K> ch;
+        solver::load_chain<K>(ch, a.tris, a.attribs, idx);
+        float xs[2 * K];
+#pragma unroll
+        for (int j = 0; j < 2 * K; j++) xs[j] = r.params[j];
+        const FirstDiffuse fd = a.fds[px];
+        const float eta = a.etas[r.bin];
+        const V3<float> L = solver::v3f<float>(a.pBeg), p = solver::v3f<float>(fd.p);
+        const V3<float> v0 = solver::vertex<float, K>(ch, xs, 0);
+        const float dAdwValue = solver::dadw<float, K>(L, v0 - L, p, ch, a.events, eta);
+        const V3<float> vl = solver::vertex<float, K>(ch, xs, K - 1);
+        const float cosv = fmaxf(solver::vdot(solver::vnormalize(vl - p), solver::v3f<float>(fd.ng)), 0.0f);
+        float contrib = r.throughput * a.lightIntensity / dAdwValue * cosv;
+        contrib = fminf(contrib, a.radianceClamp);
+        atomicAdd(a.spectral + (size_t)px * a.nBins + r.bin, contrib);
+    }
+}
+
+template <int K>
+static cudaError_t run(SubArgs& a, uint64_t* fronts[2], unsigned long long* counts, cudaStream_t s)
+{
+    const int grid = kNumSMs * 8;
+    k_sub_init<<<(a.nRows + kBlock - 1) / kBlock, kBlock, 0, s>>>(a, fronts[0], &counts[0]);
+    cudaError_t e = cudaGetLastError();
+    int cur = 0;
+    for (int d = 0; d <= a.maxDepth && e == cudaSuccess; d++) {
+        e = cudaMemsetAsync(&counts[cur ^ 1], 0, sizeof(unsigned long long), s);
+        if (e != cudaSuccess) break;
+        k_sub_round<K><<<grid, kBlock, 0, s>>>(a, d, fronts[cur], &counts[cur], fronts[cur ^ 1], &counts[cur ^ 1]);
+        e = cudaGetLastError();
+        cur ^= 1;
+    }
+    if (e != cudaSuccess) return e;
+    k_sub_leaves<K><<<grid * 2, kBlock, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace subdiv
+}  // namespace pz
+
+using namespace pz;
+using namespace pz::subdiv;
+
+static_assert(sizeof(pz_specular_root) == 64, "pz_specular_root layout");
+static_assert(kNumStats <= 8, "stats fit the header");
+
+namespace {
+constexpr size_t kHeader = 256;  // status | em1[2] | counts[2] | leaf count | root count | stats[7]
+}
+
+extern "C" size_t pz_subdivide_scratch_bytes(uint64_t box_capacity)
+{
+    return kHeader + 3 * (((size_t)box_capacity * sizeof(uint64_t) + 255) & ~(size_t)255);
+}
+
+extern "C" int pz_subdivide_solve(int K, uint32_t events, pz_float3 p_beg, const pz_float3* p_end_dev,
+                                  const uint32_t* tuples_dev, uint32_t n_tuples, const float* etas_dev, int n_bins,
+                                  const pz_subdiv_params* params, const pz_triangle* triangles_dev,
+                                  const pz_triangle_attrib* attribs_dev, const pz_internal_node* scene_internals_dev,
+                                  const pz_triangle* scene_triangles_dev, const uint32_t* scene_root_dev,
+                                  pz_specular_root* roots_dev, uint64_t root_capacity, uint64_t* n_roots_out,
+                                  pz_subdiv_stats* stats_out, void* scratch_dev, size_t scratch_bytes,
+                                  pz_stream_t stream)
+{
+    if (K < 1 || K > 4) return fail(PZ_ERR_INVALID_ARGUMENT, "pz_subdivide_solve: K must be 1..4 (got %d)", K);
+    if (!n_roots_out || !params)
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_subdivide_solve: n_roots_out and params are required");
+    *n_roots_out = 0;
+    if (stats_out) *stats_out = pz_subdiv_stats{};
+    if (params->max_depth < 0 || params->max_depth > kMaxDepth)
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_subdivide_solve: max_depth must be 0..%d (got %d)", kMaxDepth,
+                    params->max_depth);
+    if (n_bins < 1 || n_bins > kMaxBins)
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_subdivide_solve: n_bins must be 1..%d (got %d)", kMaxBins, n_bins);
+    if (!(params->eps >= 0.0f) || params->max_iterations < 1)
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_subdivide_solve: bad eps or max_iterations");
+    if (n_tuples == 0) {
+        clear_error();
+        return PZ_OK;
+    }
+    if (!p_end_dev || !tuples_dev || !etas_dev || !triangles_dev || !attribs_dev || !scene_internals_dev ||
+        !scene_triangles_dev || !scene_root_dev || !scratch_dev || (root_capacity > 0 && !roots_dev))
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_subdivide_solve: null buffer");
+    if (reinterpret_cast<uintptr_t>(scratch_dev) & 255)
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_subdivide_solve: scratch needs 256-byte alignment");
+    if (scratch_bytes < pz_subdivide_scratch_bytes(n_tuples))
+        return fail(PZ_ERR_SCRATCH_TOO_SMALL, "pz_subdivide_solve: scratch %zu < %zu (a frontier must hold the tuples)",
+                    scratch_bytes, pz_subdivide_scratch_bytes(n_tuples));
+    const size_t part = ((scratch_bytes - kHeader) / 3) & ~(size_t)255;
+    char* base = static_cast<char*>(scratch_dev);
+    uint32_t* status = reinterpret_cast<uint32_t*>(base);
+    float* em1 = reinterpret_cast<float*>(base + 8);
+    unsigned long long* counts = reinterpret_cast<unsigned long long*>(base + 16);  // [2]
+    unsigned long long* nLeaves = reinterpret_cast<unsigned long long*>(base + 32);
+    unsigned long long* nRoots = reinterpret_cast<unsigned long long*>(base + 40);
+    unsigned long long* stats = reinterpret_cast<unsigned long long*>(base + 48);  // [kNumStats]
+    uint64_t* fronts[2] = {reinterpret_cast<uint64_t*>(base + kHeader),
+                           reinterpret_cast<uint64_t*>(base + kHeader + part)};
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+
+    SubArgs a;
+    a.events = events;
+    a.pBeg = make_float3(p_beg.x, p_beg.y, p_beg.z);
+    a.pEnd = reinterpret_cast<const float3*>(p_end_dev);
+    a.tuples = tuples_dev;
+    a.nRows = n_tuples;
+    a.etas = etas_dev;
+    a.nBins = (uint32_t)n_bins;
+    a.maxDepth = params->max_depth;
+    a.eps = params->eps;
+    a.maxIterations = params->max_iterations;
+    a.costTolerance = params->cost_tolerance;
+    a.warmUp = params->early_term_warmup;
+    a.polish = params->fp64_polish;
+    a.tris = reinterpret_cast<const Tri*>(triangles_dev);
+    a.attribs = reinterpret_cast<const Attrib*>(attribs_dev);
+    a.nodes = reinterpret_cast<const Node*>(scene_internals_dev);
+    a.sceneTris = reinterpret_cast<const Tri*>(scene_triangles_dev);
+    a.root = scene_root_dev;
+    a.capacity = part / sizeof(uint64_t);
+    a.em1 = em1;
+    a.leaves = reinterpret_cast<uint64_t*>(base + kHeader + 2 * part);
+    a.nLeaves = nLeaves;
+    a.roots = roots_dev;
+    a.nRoots = nRoots;
+    a.rootCapacity = root_capacity;
+    a.stats = stats;
+    a.status = status;
+
+    cudaError_t e = cudaMemsetAsync(base, 0, kHeader, s);
+    if (e == cudaSuccess) {
+        switch (K) {
+            case 1: e = run<1>(a, fronts, counts, s); break;
+            case 2: e = run<2>(a, fronts, counts, s); break;
+            case 3: e = run<3>(a, fronts, counts, s); break;
+            default: e = run<4>(a, fronts, counts, s); break;
+        }
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "pz_subdivide_solve: launch");
+    unsigned long long hdr[6 + kNumStats];
+    e = cudaMemcpyAsync(hdr, base, sizeof(hdr), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e, "pz_subdivide_solve: results");
+    const uint32_t st = (uint32_t)(hdr[0] & 0xFFFFFFFFull);
+    *n_roots_out = hdr[5];
+    if (stats_out) {
+        stats_out->boxes_tested = hdr[6 + kStTested];
+        stats_out->boxes_culled = hdr[6 + kStCulled];
+        stats_out->leaves = hdr[4];
+        stats_out->solves = hdr[6 + kStSolves];
+        stats_out->converged = hdr[6 + kStConverged];
+        stats_out->outside_box = hdr[6 + kStOutside];
+        stats_out->roots = hdr[6 + kStRoots];
+        stats_out->polished = hdr[6 + kStPolished];
+    }
+    if (st & kErrCapacity)
+        return fail(PZ_ERR_DEVICE, "pz_subdivide_solve: capacity exceeded (%llu roots for %llu slots, or the box lists)",
+                    (unsigned long long)hdr[5], (unsigned long long)root_capacity);
+    clear_error();
+    return PZ_OK;
+}
+
+extern "C" int pz_subdivide_contribute(int K, uint32_t events, pz_float3 p_beg, float light_intensity,
+                                       float radiance_clamp, const uint32_t* tuples_dev,
+                                       const pz_specular_root* roots_dev, uint64_t n_roots,
+                                       const void* first_diffuse_dev, const float* etas_dev, int n_bins,
+                                       const pz_triangle* triangles_dev, const pz_triangle_attrib* attribs_dev,
+                                       float* spectral_dev, pz_stream_t stream)
+{
+    if (K < 1 || K > 4) return fail(PZ_ERR_INVALID_ARGUMENT, "pz_subdivide_contribute: K must be 1..4 (got %d)", K);
+    if (n_bins < 1 || n_bins > kMaxBins)
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_subdivide_contribute: n_bins must be 1..%d", kMaxBins);
+    if (n_roots == 0) {
+        clear_error();
+        return PZ_OK;
+    }
+    if (!tuples_dev || !roots_dev || !first_diffuse_dev || !etas_dev || !triangles_dev || !attribs_dev ||
+        !spectral_dev)
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_subdivide_contribute: null buffer");
+    ContribArgs a;
+    a.events = events;
+    a.pBeg = make_float3(p_beg.x, p_beg.y, p_beg.z);
+    a.lightIntensity = light_intensity;
+    a.radianceClamp = radiance_clamp;
+    a.tuples = tuples_dev;
+    a.roots = roots_dev;
+    a.nRoots = n_roots;
+    a.fds = static_cast<const FirstDiffuse*>(first_diffuse_dev);
+    a.etas = etas_dev;
+    a.nBins = (uint32_t)n_bins;
+    a.tris = reinterpret_cast<const Tri*>(triangles_dev);
+    a.attribs = reinterpret_cast<const Attrib*>(attribs_dev);
+    a.spectral = spectral_dev;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const unsigned grid = (unsigned)std::min<uint64_t>((n_roots + kBlock - 1) / kBlock, (uint64_t)kNumSMs * 16);
+    switch (K) {
+        case 1: k_sub_contribute<1><<<grid, kBlock, 0, s>>>(a); break;
+        case 2: k_sub_contribute<2><<<grid, kBlock, 0, s>>>(a); break;
+        case 3: k_sub_contribute<3><<<grid, kBlock, 0, s>>>(a); break;
+        default: k_sub_contribute<4><<<grid, kBlock, 0, s>>>(a); break;
+    }
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "pz_subdivide_contribute");
+    clear_error();
+    return PZ_OK;
+}

@@ -37,6 +37,21 @@ def event_descriptor(events: str) -> int:
     return bits | (len(events) << 24)
 
 
+_R2_G = 1.32471795724474602596  # plastic number, x^3 = x + 1
+
+
+def light_point(center, size, iteration: int) -> tuple:
+    """Sample `iteration` of a square light (Scene.light_point); the same arithmetic as
+    palzilla_b200::light_point in include/palzilla_b200.hpp (double, rounded to float)."""
+    c = [float(np.float32(x)) for x in center]
+    sx, sz = float(np.float32(size[0])), float(np.float32(size[1]))
+    if sx == 0.0 and sz == 0.0:
+        return tuple(c)
+    u = math.fmod(0.5 + iteration / _R2_G, 1.0)
+    v = math.fmod(0.5 + iteration / (_R2_G * _R2_G), 1.0)
+    return (float(np.float32(c[0] + (u - 0.5) * sx)), c[1], float(np.float32(c[2] + (v - 0.5) * sz)))
+
+
 @dataclasses.dataclass
 class Camera:
     eye: tuple
@@ -51,6 +66,7 @@ class Scene:
     tris: np.ndarray      # (n, 9) float32
     attribs: np.ndarray   # (n,) ATTRIB_DTYPE
     p_light: tuple = (0.0, 3.0, 0.0)
+    light_size: tuple = (0.0, 0.0)   # extent along x and z of a downward-facing square light
     camera: Camera | None = None
     width: int = 256
     height: int = 256
@@ -70,6 +86,14 @@ class Scene:
     @property
     def n(self) -> int:
         return int(self.tris.shape[0])
+
+    def light_point(self, iteration: int) -> tuple:
+        """The point light that stands for the area light at this iteration: the square
+        light_size centred on p_light, sampled by the R2 sequence (Roberts 2018:
+        x_i = frac(1/2 + i / g), y_i = frac(1/2 + i / g^2), g the plastic number), one
+        sample per iteration.  Iteration 0 is the centre; a light of size zero is the
+        point p_light."""
+        return light_point(self.p_light, self.light_size, iteration)
 
     def bin_lambdas(self) -> np.ndarray:
         w = (self.lambda_max - self.lambda_min) / self.n_bins
@@ -261,16 +285,17 @@ def adjoint_scene(side: int = 128, seed: int = 1, width: int = 512, height: int 
     return sc, corners, heights
 
 
-def sphere_scene(subdivisions: int = 5, n_bins: int = 64, width: int = 1024, height: int = 1024) -> Scene:
+def sphere_scene(subdivisions: int = 5, n_bins: int = 64, width: int = 1024, height: int = 1024,
+                 light_size=(0.2, 0.2)) -> Scene:
     """Two-refraction dispersive sphere: icosphere r=0.5 at (0,1,0) over a 4x4 receiver at
-    y=0.  The light sits at (0,4,0) (centre of the 0.2 x 0.2 area light).  The camera at
-    y=0.45, below the sphere, looks down on the central 0.9 x 0.9 of the receiver where
-    the caustic falls."""
+    y=0, lit by a 0.2 x 0.2 area light centred at (0,4,0), one point sample of it per
+    iteration (Scene.light_point).  The camera at y=0.45, below the sphere, looks down on
+    the central 0.9 x 0.9 of the receiver where the caustic falls."""
     sph = icosphere(subdivisions)
     tris, att = _combine([sph, receiver_plane(4.0, 0.0)])
     cam = Camera(eye=(0.0, 0.45, 0.0), center=(0.0, 0.0, 0.0), up=(0.0, 0.0, -1.0), fovy=math.pi / 2)
-    return Scene(name=f"sphere{subdivisions}", tris=tris, attribs=att, p_light=(0.0, 4.0, 0.0), camera=cam,
-                 events="TT", n_bins=n_bins, width=width, height=height)
+    return Scene(name=f"sphere{subdivisions}", tris=tris, attribs=att, p_light=(0.0, 4.0, 0.0), light_size=light_size,
+                 camera=cam, events="TT", n_bins=n_bins, width=width, height=height)
 
 
 def uneven_batch(n_scenes: int = 256, seed: int = 3001, side_min: int = 16, side_max: int = 256, width: int = 256,

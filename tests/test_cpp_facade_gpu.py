@@ -2,7 +2,8 @@
 RayGenerator) driven by a C++ program (palzilla_b200/pk_render) renders the same image as
 the same sequence of C-ABI calls made from Python: two iterations of the reference's
 step() (eye pass, photon pass, and lookup / sort / reorder / plain solve for the event
-strings T, R, TT, TTTT, TRT, TTT) on a two-sheet heightfield lens."""
+strings T, R, TT, TTTT, TRT, TTT) on a two-sheet heightfield lens under a square area
+light, sampled at one point per iteration on both sides."""
 import os
 import struct
 import subprocess
@@ -35,7 +36,7 @@ def _python_render(sc, iterations):
             if n == 0:
                 continue
             A.sort_and_reorder(frame, n, sorter)
-            A.solve_specular_plain(A.solve_desc(ds, frame, cache, ev, n))
+            A.solve_specular_plain(A.solve_desc(ds, frame, cache, ev, n, iteration=it))
             solved += n
     pixels = torch.empty(sc.width * sc.height, dtype=torch.int32, device="cuda")
     A._lib.call("pz_resolve", A._vp(pixels), A._vp(frame.accum), sc.width * sc.height, None)
@@ -46,13 +47,14 @@ def _python_render(sc, iterations):
 def test_pk_renderer_matches_c_abi_sequence(tmp_path):
     exe = B.build_pk_render()
     sc = S.lens_scene(side=32, seed=3, width=96, height=96, n_bins=1, events="TT")
+    sc.light_size = (0.1, 0.1)  # an area light: each iteration samples another point of it
     iterations = 2
     cam = sc.camera
     path_in, path_out = tmp_path / "scene.bin", tmp_path / "out.bin"
     with open(path_in, "wb") as f:
         f.write(struct.pack("<4i", sc.n, sc.width, sc.height, iterations))
         f.write(struct.pack("<10f", *cam.eye, *cam.center, *cam.up, cam.fovy))
-        f.write(struct.pack("<3f", *sc.p_light))
+        f.write(struct.pack("<5f", *sc.p_light, *sc.light_size))
         f.write(struct.pack("<5f", sc.light_intensity, sc.radiance_clamp, sc.min_throughput, sc.cauchy_a, sc.cauchy_b))
         f.write(np.ascontiguousarray(sc.tris, np.float32).tobytes())
         f.write(np.ascontiguousarray(sc.attribs).tobytes())

@@ -209,3 +209,82 @@ def test_live_render_vs_reference(orc, ref):
     ir, sr = ref.render_pairs(2, pairs, cache, fd, bvh, sc, sc.bin_etas())
     assert io.tobytes() == ir.tobytes() and np.array_equal(so, sr)
     assert so[2] > 0
+
+
+def test_subdivision_finds_every_root_of_dense_starts(orc):
+    """The subdivision solve (pz_oracle_subdiv.hpp, the checker of pz_subdivide_solve) has no
+    reference counterpart; it is pinned by a property: every contributing root that the
+    reference's Newton solve (solveConstraints<K>, pk.h:466-592) reaches from a dense grid
+    of starts in any (receiver point, lens triangle) domain is among its roots, and it
+    reports no root the grid does not find (within 1e-3 in the barycentrics: roots of
+    ill-conditioned tuples stop anywhere in a 1e-4-wide basin)."""
+    sc = S.lens_scene(side=8, seed=5, amplitude=0.05, events="T", width=16, height=16)
+    ev = S.event_descriptor("T")
+    bvh = orc.build_bvh(sc.tris, 0)
+    rng = np.random.default_rng(2)
+    ends = rng.uniform(-0.4, 0.4, (6, 3)).astype(np.float32)
+    ends[:, 1] = 0.0
+    spec = np.nonzero(sc.attribs["material"] != 0)[0]
+    rows = np.array([[q, i] for q in range(len(ends)) for i in spec], np.uint32)
+    roots, stats = orc.subdivide_solve(1, ev, sc.p_light, ends, rows, np.array([1.5], np.float32), sc.tris, sc.attribs,
+                                       bvh, sc.tris)
+    assert stats[1] > len(rows) // 2 and len(roots) > 10
+    sub = {}
+    for r in roots:
+        sub.setdefault(int(r["tuple"]), []).append(r["params"][:2])
+    grid = [(u, v) for u in np.linspace(0.02, 0.98, 9) for v in np.linspace(0.02, 0.98, 9) if u + v <= 1.0]
+    brute = {}
+    for ri, (q, tri) in enumerate(rows):
+        T, At = sc.tris[[tri]], sc.attribs[[tri]]
+        for u, v in grid:
+            ok, p, _ = orc.solve_constraints(1, np.array([u, v], np.float32), sc.p_light, ends[q], T, At, 1.5, ev)
+            if ok and orc.contributable_throughput(1, p, sc.p_light, ends[q], T, At, ev, bvh, sc.tris, 1.5) > 0:
+                lst = brute.setdefault(ri, [])
+                if not any(np.abs(p - x).max() < 1e-4 for x in lst):
+                    lst.append(p)
+    for ri in set(sub) | set(brute):
+        a, b = sub.get(ri, []), brute.get(ri, [])
+        assert all(any(np.abs(p - x).max() < 1e-3 for x in a) for p in b), ri
+        assert all(any(np.abs(p - x).max() < 1e-3 for p in b) for x in a), ri
+
+
+def _f32_neighbours(x):
+    """The float32 values just below and above the exact rational x (equal when x is one)."""
+    from fractions import Fraction
+    f = np.float32(float(x))  # round to nearest double, then to float: within one float step
+    lo, hi = f, f
+    while Fraction(float(lo)) > x:
+        lo = np.nextafter(lo, np.float32(-np.inf))
+    while Fraction(float(hi)) < x:
+        hi = np.nextafter(hi, np.float32(np.inf))
+    while Fraction(float(np.nextafter(lo, np.float32(np.inf)))) <= x:
+        lo = np.nextafter(lo, np.float32(np.inf))
+    while Fraction(float(np.nextafter(hi, np.float32(-np.inf)))) >= x:
+        hi = np.nextafter(hi, np.float32(-np.inf))
+    return float(lo), float(hi)
+
+
+def test_subdivision_directed_rounding_is_exact(orc):
+    """The oracle's directed rounding (error-free transformations, no FPU mode switch) gives
+    the IEEE round-down / round-up results the GPU intrinsics give: checked against exact
+    rational arithmetic on random floats of mixed magnitudes (results within the float
+    range), subnormals included."""
+    from fractions import Fraction
+    rng = np.random.default_rng(9)
+    vals = np.concatenate([rng.standard_normal(300) * 10.0 ** rng.integers(-18, 18, 300),
+                           rng.standard_normal(50) * 1e-40, [0.0, 1.0, -1.0, 2.0 ** -149, 3.0, 0.1]])
+    vals = vals.astype(np.float32)
+    pairs = rng.choice(vals, (1500, 2))
+    for a, b in pairs:
+        a, b = float(a), float(b)
+        for op, exact in ((0, Fraction(a) + Fraction(b)), (1, Fraction(a) - Fraction(b)), (2, Fraction(a) * Fraction(b))):
+            lo, hi = _f32_neighbours(exact)
+            assert orc.directed(op, False, a, b) == lo and orc.directed(op, True, a, b) == hi, (op, a, b)
+        if b != 0.0 and abs(a / b) < 1e37:
+            lo, _ = _f32_neighbours(Fraction(a) / Fraction(b))
+            assert orc.directed(3, False, a, b) == lo, (a, b)
+        x = abs(a)
+        d, u = orc.directed(4, False, x), orc.directed(4, True, x)
+        assert Fraction(d) ** 2 <= Fraction(x) <= Fraction(u) ** 2
+        assert u == d or u == float(np.nextafter(np.float32(d), np.float32(np.inf)))
+        assert (u == d) == (Fraction(d) ** 2 == Fraction(x))
