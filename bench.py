@@ -552,6 +552,86 @@ def run_pathcuts(args):
           flush=True)
 
 
+def run_subdivision(args):
+    """Subdivision workload: the single-refraction heightfield lens (64 x 64 vertices, 7,938
+    lens triangles), 256 x 256 image, 16 bins, point light at (0,3,0).  The photon pass's
+    work list -- one row per (pixel, cached tuple) -- is solved by per-tuple domain
+    subdivision (depth limit 12, eps 1e-4, affine bounds with directed rounding) and the
+    roots go to the binned spectral image; each step is pz_subdivide_solve +
+    pz_subdivide_contribute on inputs already in HBM.  The single-start plain solve of the
+    same work list is timed beside it, and the CPU oracle of the subdivision on a sample of
+    the rows."""
+    import torch
+    from palzilla_b200 import api as A
+    from palzilla_b200 import scenes as S
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    sc = S.lens_scene(side=64, seed=1, width=256, height=256, n_bins=16, events="T")
+    ds = A.DeviceScene(sc)
+    frame = A.Frame(sc, path_capacity=1 << 24)
+    cache = A.PathCache(capacity=1 << 22, step=sc.cell_step)
+    ev = S.event_descriptor("T")
+    A.solve_primary(ds, frame, iteration=0)
+    A.photon_trace(ds, cache, iteration=0)
+    n = A.lookup_flatten(frame, cache, ev)
+    A.sort_and_reorder(frame, n, A.OnesweepSort())
+    rows = A.work_list_rows(frame, cache, n, 1)
+    ends = A.receiver_points(frame)
+    etas = torch.from_numpy(sc.bin_etas()).cuda()
+    spectral = torch.zeros((sc.width * sc.height, sc.n_bins), device="cuda")
+    solver = A.SubdivisionSolver(box_capacity=1 << 25, root_capacity=1 << 24)
+
+    def step():
+        spectral.zero_()
+        _, _, _, st = solver.run(1, ev, sc.light_point(0), ends, rows, etas, ds.tris, ds.attribs, ds.builder, ds.tris)
+        solver.contribute(1, ev, sc, rows, st["roots"], frame, etas, ds.tris, ds.attribs, spectral)
+        return st
+
+    for _ in range(args.warmup):
+        st = step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        st = step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    plain = torch.zeros_like(spectral)
+    d = A.solve_desc(ds, frame, cache, "T", n, spectral=plain, etas=etas)
+    A.solve_specular_plain(d)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        A.solve_specular_plain(d)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_plain = e0.elapsed_time(e1) / args.steps
+    cpu = None
+    if not args.no_cpu:
+        import oracle as O
+        orc = O.oracle()
+        bo = orc.build_bvh(sc.tris, 0)
+        rows_h, ends_h = rows.cpu().numpy(), ends.cpu().numpy()
+        sample = rows_h[:: max(1, len(rows_h) // 20000)]
+        t0 = time.perf_counter()
+        _, cst = orc.subdivide_solve(1, ev, sc.light_point(0), ends_h, sample, sc.bin_etas(), sc.tris, sc.attribs, bo,
+                                     sc.tris)
+        dt = time.perf_counter() - t0
+        cpu = {"value": float(cst[3]) / dt, "unit": "leaf Newton solves/s", "cores": orc.max_threads(), "kind": "port",
+               "sample": f"{len(sample)} of the {n} work items, all bins, {dt:.1f} s"}
+    print(json.dumps({"metric": "subdivision solve: leaf Newton solves/s and ms per work list",
+                      "workload": "subdivision", "value": st["solves"] / (ms / 1e3), "unit": "leaf Newton solves/s",
+                      "higher_is_better": True, "data": "synthetic", "dtype": "f32",
+                      "config": {"workload": "single-refraction heightfield lens", "triangles": sc.n,
+                                 "image": "256x256", "bins": sc.n_bins, "max_depth": 12, "eps": 1e-4},
+                      "work_items": n, "ms_per_step": ms, "stats": st,
+                      "roots_per_s": st["roots"] / (ms / 1e3), "boxes_per_s": st["boxes_tested"] / (ms / 1e3),
+                      "plain_single_start_ms": ms_plain,
+                      "image_energy_subdivision_over_single_start": float(spectral.sum() / plain.sum()),
+                      "cpu_baseline": cpu}),
+          flush=True)
+
+
 def run_adjoint(args):
     """Adjoint workload: 128 x 128 heightfield lens (32,258 triangles), 512 x 512 image, 8
     bins, L2 loss against a second seeded heightfield: forward (exact-arithmetic binned
@@ -705,9 +785,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-sort", action="store_true")
     ap.add_argument("--workload", default="sphere", choices=["sphere", "sort_build", "uneven_batch", "pathcuts",
-                                                             "adjoint"],
+                                                             "adjoint", "subdivision"],
                     help="sphere: the frame benchmark; sort_build: onesweep sort + LBVH build alone; "
-                         "uneven_batch: 256 heightfield lenses of uneven size per frame")
+                         "uneven_batch: 256 heightfield lenses of uneven size per frame; subdivision: per-tuple "
+                         "domain subdivision of the lens work list")
     ap.add_argument("--batch-scenes", type=int, default=256)
     ap.add_argument("--cuts-sample", type=int, default=64)
     ap.add_argument("--sizes", default="20,22,24", help="log2 sizes of the sort_build workload")
@@ -720,6 +801,8 @@ def main():
         run_pathcuts(args)
     elif args.workload == "adjoint":
         run_adjoint(args)
+    elif args.workload == "subdivision":
+        run_subdivision(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
