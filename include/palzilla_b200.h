@@ -314,7 +314,8 @@ PZ_API int pz_path_cuts(int K, uint32_t events, float eta, pz_float3 p_beg, cons
  * zero, that lie outside a triangle or whose cosines rule the event out are dropped.
  * A box stops splitting at max_depth, or when every bounded residual component is
  * narrower than eps; its centre starts the Newton solve for each wavelength bin
- * (eta = etas_dev[bin]; the bins share one subdivision).  A root is kept when it
+ * (eta = etas_dev[bin]; the bins share one subdivision, with eta^2 - 1 as one more noise
+ * symbol) whose residual, with that bin's eta substituted, may vanish in the box.  A root is kept when it
  * converged, lies in its own box (each root has one owner box) and
  * contributableThroughput (pk.h:760-842) is positive.  The tuple rows index
  * triangles_dev / attribs_dev (the specular soup pz_path_cuts ran on, or the scene);
@@ -329,7 +330,9 @@ typedef struct pz_subdiv_params {
     int fp64_polish;       /* 0; 1 = 4 FP64 Newton steps on every root found in its box */
 } pz_subdiv_params;
 typedef struct pz_subdiv_stats {
-    uint64_t boxes_tested, boxes_culled, leaves, solves, converged, outside_box, roots, polished;
+    uint64_t boxes_tested, boxes_culled, leaves;
+    uint64_t bins_excluded; /* (leaf, bin) pairs whose residual for that bin excludes zero */
+    uint64_t solves, converged, outside_box, roots, polished;
 } pz_subdiv_stats;
 typedef struct pz_specular_root {
     uint32_t tuple;   /* row of tuples_dev */
@@ -341,7 +344,8 @@ typedef struct pz_specular_root {
     uint32_t pad[3];
 } pz_specular_root;   /* 64 bytes */
 /* Scratch: a 256-byte header, two box frontiers and the leaf list of box_capacity entries
- * each (box_capacity >= n_tuples). */
+ * each (box_capacity >= n_tuples); the frontiers then hold the (leaf, bin) solve list
+ * (2 * box_capacity entries). */
 PZ_API size_t pz_subdivide_scratch_bytes(uint64_t box_capacity);
 /* Writes the kept roots (unordered) to roots_dev and their count (which may exceed
  * root_capacity: PZ_ERR_DEVICE is then returned) to *n_roots_out.  Synchronises `stream`

@@ -338,12 +338,12 @@ class CpuLib:
     def subdivide_solve(self, K, ev, p_beg, p_end, tuples, etas, tris, attribs, bvh, scene_tris, max_depth=12,
                         eps=1e-4, max_iterations=32, cost_tolerance=1e-10, warm_up=1, cap=1 << 20):
         """Roots of the subdivision solve, sorted by (tuple, bin, depth, path), and the stats
-        (tested, culled, leaves, solves, converged, outside, roots).  tuples index
-        tris / attribs; visibility runs through bvh over scene_tris."""
+        (tested, culled, leaves, bins excluded, solves, converged, outside, roots).  tuples
+        index tris / attribs; visibility runs through bvh over scene_tris."""
         tuples = np.ascontiguousarray(tuples, np.uint32)
         etas = np.ascontiguousarray(etas, np.float32)
         out = np.zeros(cap, ROOT_DTYPE)
-        stats = np.zeros(7, np.uint64)
+        stats = np.zeros(8, np.uint64)
         n = self.f("subdivide_solve", C.c_int64)(
             C.c_int(K), C.c_uint32(ev), _p(np.asarray(p_beg, np.float32)), _p(np.ascontiguousarray(p_end, np.float32)),
             _p(tuples), C.c_uint32(len(tuples)), _p(etas), C.c_int(len(etas)), C.c_int(max_depth), C.c_float(eps),

@@ -595,8 +595,9 @@ int64_t pzo_path_cuts(int K, uint32_t events, float eta, const float* p_beg, con
 
 // Subdivision solve (pz_oracle_subdiv.hpp): roots of every tuple row {q, tri[0..K)},
 // sorted by (tuple, bin, depth, path).  The rows index tris / attribs; visibility runs
-// through nodes over scene_tris.  stats[7]: boxes tested, culled, leaves, solves,
-// converged, outside their box, roots.  Returns the root count (negative on overflow).
+// through nodes over scene_tris.  stats[8]: boxes tested, culled, leaves, (leaf, bin)
+// pairs excluded, solves, converged, outside their box, roots.  Returns the root count
+// (negative on overflow).
 int64_t pzo_subdivide_solve(int K, uint32_t events, const float* p_beg, const float* p_end, const uint32_t* tuples,
                             uint32_t n_tuples, const float* etas, int n_bins, int max_depth, float eps,
                             int max_iterations, float cost_tolerance, int warm_up, const Triangle* tris,
@@ -607,7 +608,7 @@ int64_t pzo_subdivide_solve(int K, uint32_t events, const float* p_beg, const fl
     const F3 a = ld3(p_beg);
     const F3* ends = reinterpret_cast<const F3*>(p_end);
     std::vector<std::vector<subdiv::Root>> rows(n_tuples);
-    std::vector<std::array<uint64_t, 7>> st(n_tuples);
+    std::vector<std::array<uint64_t, 8>> st(n_tuples);
 #pragma omp parallel for schedule(dynamic, 4)
     for (int64_t r = 0; r < (int64_t)n_tuples; r++) {
         st[r].fill(0);
@@ -622,9 +623,9 @@ int64_t pzo_subdivide_solve(int K, uint32_t events, const float* p_beg, const fl
     }
     int64_t n = 0;
     subdiv::Root* o = static_cast<subdiv::Root*>(out);
-    for (int j = 0; j < 7; j++) stats[j] = 0;
+    for (int j = 0; j < 8; j++) stats[j] = 0;
     for (uint32_t r = 0; r < n_tuples; r++) {
-        for (int j = 0; j < 7; j++) stats[j] += st[r][j];
+        for (int j = 0; j < 8; j++) stats[j] += st[r][j];
         auto& v = rows[r];
         std::sort(v.begin(), v.end(), [](const subdiv::Root& x, const subdiv::Root& y) {
             return std::make_tuple(x.bin, x.depth, x.path) < std::make_tuple(y.bin, y.depth, y.path);

@@ -10,10 +10,12 @@
 //     the event out (the test of contributableThroughput, pk.h:760-842), or when an
 //     affine bound of the residual of solveConstraints<K> (pk.h:466-592; cross product of
 //     the outgoing direction with the reflected / refracted one) excludes zero;
+//   - eta^2 - 1 over the bins is one more noise symbol of the bound;
 //   - a box stops splitting at max_depth or when every bounded residual component is
-//     narrower than eps; its centre then starts the Newton solve (solve_constraints in
-//     pz_oracle.hpp) for every bin, and the root is kept when it converged, lies in the
-//     box (half-open) and its contributable throughput is positive.
+//     narrower than eps; at such a leaf every bin's value of eta^2 - 1 is substituted
+//     into the residual forms, and for the bins whose residual may vanish the box centre
+//     starts the Newton solve (solve_constraints in pz_oracle.hpp); a root is kept when it
+//     converged, lies in the box (half-open) and its contributable throughput is positive.
 // Affine arithmetic: central and linear coefficients round to nearest, every rounding
 // error and nonlinear remainder is added to the radius rounded upward.
 //
@@ -65,6 +67,12 @@ inline float div_d(float a, float b)
     const float q = a / b;
     const double rem = std::fma(-(double)q, (double)b, (double)a);  // a - q b, exact
     return (rem < 0.0) != (b < 0.0) && rem != 0.0 ? dn(q) : q;
+}
+inline float div_u(float a, float b)
+{
+    const float q = a / b;
+    const double rem = std::fma(-(double)q, (double)b, (double)a);
+    return (rem > 0.0) == (b > 0.0) && rem != 0.0 ? up(q) : q;
 }
 inline float sqrt_u(float a)
 {
@@ -200,11 +208,19 @@ inline void box_bounds(int N, uint32_t path, int depth, float* l, float* h)
 
 enum { kCull = 0, kSplit = 1, kLeaf = 2 };
 
+// one vertex's residual over a box: per component the centre, the radius without the
+// eta^2 - 1 symbol, and that symbol's coefficient
+struct VertexForms {
+    bool valid;
+    float c[3], rad[3], xe[3];
+};
+
+// Noise symbols 0 .. 2K-1: the box's parameters; symbol 2K: eta^2 - 1 over the bins.
 template <int K>
-int bound_box(const Triangle* tris, const TriangleAttrib* attribs, F3 pBeg, F3 pEnd, uint32_t events, const Af<2 * K>& em1,
-              const float* bl, const float* bh, float eps)
+int bound_box(const Triangle* tris, const TriangleAttrib* attribs, F3 pBeg, F3 pEnd, uint32_t events, const Af<2 * K + 1>& em1,
+              const float* bl, const float* bh, float eps, VertexForms* forms = nullptr)
 {
-    constexpr int N = 2 * K;
+    constexpr int N = 2 * K + 1;
     for (int k = 0; k < K; k++)
         if (add_d(bl[2 * k], bl[2 * k + 1]) > 1.0f) return kCull;
     Af3<N> X[K + 2], Nrm[K];
@@ -224,6 +240,7 @@ int bound_box(const Triangle* tris, const TriangleAttrib* attribs, F3 pBeg, F3 p
     }
     bool resolved = true;
     for (int k = 0; k < K; k++) {
+        if (forms) forms[k].valid = false;
         Af3<N> wi = sub3(X[k], X[k + 1]);
         Af3<N> wo = sub3(X[k + 2], X[k + 1]);
         const Af3<N>& n = Nrm[k];
@@ -259,9 +276,49 @@ int bound_box(const Triangle* tris, const TriangleAttrib* attribs, F3 pBeg, F3 p
             const float l = lo(*cc[j]), h = hi(*cc[j]);
             if (l > 0.0f || h < 0.0f) return kCull;
             resolved = resolved && sub_u(h, l) < eps;
+            if (forms) {
+                float r = cc[j]->r;
+                for (int i = 0; i < N - 1; i++) r = add_u(r, std::fabs(cc[j]->x[i]));
+                forms[k].c[j] = cc[j]->c;
+                forms[k].rad[j] = r;
+                forms[k].xe[j] = cc[j]->x[N - 1];
+            }
         }
+        if (forms) forms[k].valid = true;
     }
     return resolved ? kLeaf : kSplit;
+}
+
+template <int M> Af<M> em1_form(float mLo, float mHi)
+{
+    Af<M> e = cst<M>((mLo + mHi) * 0.5f);
+    e.x[M - 1] = std::fmax(sub_u(mHi, e.c), sub_u(e.c, mLo));
+    return e;
+}
+
+// can a root for the bin value m of eta^2 - 1 lie in the box (the leaf test)?
+template <int K>
+bool bin_may_hold_root(const VertexForms* forms, const Af<2 * K + 1>& em1, float m)
+{
+    constexpr int M = 2 * K + 1;
+    const float rad = em1.x[M - 1];
+    float elo = 0.0f, ehi = 0.0f;
+    if (rad > 0.0f) {
+        elo = div_d(sub_d(m, em1.c), rad);
+        ehi = div_u(sub_u(m, em1.c), rad);
+    }
+    for (int k = 0; k < K; k++) {
+        if (!forms[k].valid) continue;
+        for (int j = 0; j < 3; j++) {
+            const float xe = forms[k].xe[j];
+            const float pl = std::fmin(mul_d(xe, elo), mul_d(xe, ehi));
+            const float ph = std::fmax(mul_u(xe, elo), mul_u(xe, ehi));
+            const float l = sub_d(add_d(forms[k].c[j], pl), forms[k].rad[j]);
+            const float h = add_u(add_u(forms[k].c[j], ph), forms[k].rad[j]);
+            if (l > 0.0f || h < 0.0f) return false;
+        }
+    }
+    return true;
 }
 
 struct Root {
@@ -280,7 +337,7 @@ struct Params {
     int warmUp;
 };
 
-// stats: tested, culled, leaves, solves, converged, outside, roots
+// stats: tested, culled, leaves, bins excluded, solves, converged, outside, roots
 template <int K>
 void solve_row(uint32_t row, const uint32_t* tuples, uint32_t events, F3 pBeg, const F3* pEnd, const float* etas, int nBins,
                const Params& P, const Triangle* soupTris, const TriangleAttrib* soupAttribs, const InternalNode* nodes,
@@ -301,8 +358,7 @@ void solve_row(uint32_t row, const uint32_t* tuples, uint32_t events, F3 pBeg, c
         mLo = b == 0 ? m : std::fmin(mLo, m);
         mHi = b == 0 ? m : std::fmax(mHi, m);
     }
-    Af<N> em1 = cst<N>((mLo + mHi) * 0.5f);
-    em1.r = std::fmax(sub_u(mHi, em1.c), sub_u(em1.c, mLo));
+    const Af<N + 1> em1 = em1_form<N + 1>(mLo, mHi);
     std::vector<std::pair<int, uint32_t>> stack{{0, 0u}};
     while (!stack.empty()) {
         const auto [depth, path] = stack.back();
@@ -319,22 +375,28 @@ void solve_row(uint32_t row, const uint32_t* tuples, uint32_t events, F3 pBeg, c
             continue;
         }
         stats[2]++;
+        VertexForms forms[K];
+        bound_box<K>(tris, attribs, pBeg, pEnd[q], events, em1, bl, bh, P.eps, forms);
         for (int b = 0; b < nBins; b++) {
+            if (!bin_may_hold_root<K>(forms, em1, etas[b] * etas[b] - 1.0f)) {
+                stats[3]++;
+                continue;
+            }
             float xs[N];
             for (int j = 0; j < N; j++) xs[j] = (bl[j] + bh[j]) * 0.5f;
             const bool conv = solve_constraints<float, K>(xs, pBeg, pEnd[q], tris, attribs, etas[b], events,
                                                           P.maxIterations, P.costTolerance, P.warmUp);
-            stats[3]++;
-            if (!conv) continue;
             stats[4]++;
+            if (!conv) continue;
+            stats[5]++;
             bool inside = true;
             for (int j = 0; j < N; j++)
                 inside = inside && bl[j] <= xs[j] && (xs[j] < bh[j] || (bh[j] == 1.0f && xs[j] == 1.0f));
-            if (!inside) { stats[5]++; continue; }
+            if (!inside) { stats[6]++; continue; }
             const float thr = contributable_throughput<float, K>(xs, pBeg, pEnd[q], tris, attribs, events, nodes,
                                                                 sceneTris, root, etas[b]);
             if (!(thr > 0.0f)) continue;
-            stats[6]++;
+            stats[7]++;
             Root r{};
             r.tuple = row;
             r.bin = (uint32_t)b;

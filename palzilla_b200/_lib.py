@@ -44,8 +44,8 @@ class SubdivParams(C.Structure):
 
 
 class SubdivStats(C.Structure):
-    _fields_ = [(n, C.c_uint64) for n in ("boxes_tested", "boxes_culled", "leaves", "solves", "converged",
-                                          "outside_box", "roots", "polished")]
+    _fields_ = [(n, C.c_uint64) for n in ("boxes_tested", "boxes_culled", "leaves", "bins_excluded", "solves",
+                                          "converged", "outside_box", "roots", "polished")]
 
 
 class SolveDesc(C.Structure):

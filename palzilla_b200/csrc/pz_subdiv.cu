@@ -15,25 +15,30 @@
 //     whole box, which contributableThroughput (pk.h:760-842) would reject.
 // A box stops splitting at the depth limit, or when every bounded residual component is
 // narrower than eps (the bound no longer tightens usefully).  Its centre then starts the
-// reference's Newton solve, once per wavelength bin.  A root is kept when
+// reference's Newton solve, once per wavelength bin that may hold a root there.  A root
+// is kept when
 //   - the solve converged,
 //   - the root lies in that box (half-open boxes: every root has one owner box, so no
 //     root is reported twice),
 //   - contributableThroughput, visibility included, is positive.
-// The wavelength bins share one subdivision: the bound takes eta^2 - 1 over the range of
-// the bins' values, so a box that survives for any bin survives.
+// The wavelength bins share one subdivision: eta^2 - 1 over the range of the bins' values
+// is one more noise symbol of the bound, so a box that survives for any bin survives.  At
+// a leaf, each bin's value of that symbol is substituted into the residual forms, and a
+// bin whose residual range then excludes zero gets no Newton solve.
 //
 // Affine forms: x = c + sum_i x_i e_i + r e_err with |e_i|, |e_err| <= 1; the noise
-// symbols e_i are the box's 2K parameters.  Central and linear coefficients are rounded
+// symbols e_i are the box's 2K parameters and eta^2 - 1.  Central and linear coefficients are rounded
 // to nearest; each rounding error, and each nonlinear remainder, goes into the radius r
 // with upward rounding, so the bound encloses the constraint in exact arithmetic.  The
 // unit is built with -fmad=false, so the CPU oracle can repeat every operation.
 //
 // Kernels: k_sub_init (one entry per tuple), k_sub_round (one launch per depth; a thread
 // per box: bound, cull, split or retire to the leaf list; warp-aggregated appends),
-// k_sub_leaves (a thread per (leaf, bin): Newton, ownership, throughput, root output),
-// k_sub_contribute (a thread per root: dAdw and the binned spectral image).  The rounds
-// read their input count on the device: no host synchronisation between launches.
+// k_sub_leaf_test (a thread per leaf: the per-bin test, surviving (leaf, bin) pairs to a
+// compact solve list), k_sub_leaf_solve (a thread per pair: Newton, ownership, throughput,
+// root output), k_sub_contribute (a thread per root: dAdw and the binned spectral image).
+// The rounds read their input count on the device: no host synchronisation between
+// launches.
 #include <algorithm>
 
 #include "pz_capi_internal.h"
@@ -52,7 +57,9 @@ constexpr int kMaxDepth = 20;  // path bits in an entry
 constexpr int kMaxBins = 256;
 constexpr uint32_t kPathMask = (1u << kMaxDepth) - 1u;
 
-enum : int { kStTested = 0, kStCulled, kStSolves, kStConverged, kStOutside, kStRoots, kStPolished, kNumStats };
+enum : int {
+    kStTested = 0, kStCulled, kStExcluded, kStSolves, kStConverged, kStOutside, kStRoots, kStPolished, kNumStats
+};
 
 // ---------------------------------------------------------------- affine forms
 // Rounding error of one round-to-nearest result r: at most |r| 2^-24 (normal) or 2^-150.
@@ -239,12 +246,20 @@ template <int N> PZ_D void box_bounds(uint32_t path, int depth, float* lo, float
 
 enum Verdict : int { kCull = 0, kSplit = 1, kLeaf = 2 };
 
-// The bound of one box.  em1: eta^2 - 1 over the bins, as an affine constant.
+// The residual of one vertex over a box, for the per-bin test of the leaves: per component
+// the centre, the radius without the eta^2 - 1 symbol, and that symbol's coefficient.
+struct VertexForms {
+    bool valid;
+    float c[3], rad[3], xe[3];
+};
+
+// The bound of one box.  Noise symbols 0 .. 2K-1 are the box's parameters, symbol 2K is
+// eta^2 - 1 over the bins (em1).  forms (may be null) receives each vertex's residual.
 template <int K>
-PZ_D int bound_box(const Chain<K>& ch, float3 pBeg, float3 pEnd, uint32_t events, const Af<2 * K>& em1,
-                   const float* lo, const float* hi, float eps)
+PZ_D int bound_box(const Chain<K>& ch, float3 pBeg, float3 pEnd, uint32_t events, const Af<2 * K + 1>& em1,
+                   const float* lo, const float* hi, float eps, VertexForms* forms = nullptr)
 {
-    constexpr int N = 2 * K;
+    constexpr int N = 2 * K + 1;
 #pragma unroll
     for (int k = 0; k < K; k++)
         if (__fadd_rd(lo[2 * k], lo[2 * k + 1]) > 1.0f) return kCull;  // outside the triangle
@@ -263,6 +278,7 @@ PZ_D int bound_box(const Chain<K>& ch, float3 pBeg, float3 pEnd, uint32_t events
     bool resolved = true;
 #pragma unroll
     for (int k = 0; k < K; k++) {
+        if (forms) forms[k].valid = false;
         Af3<N> wi = af3_sub(X[k], X[k + 1]);
         Af3<N> wo = af3_sub(X[k + 2], X[k + 1]);
         const Af3<N>& n = Nrm[k];
@@ -312,9 +328,55 @@ PZ_D int bound_box(const Chain<K>& ch, float3 pBeg, float3 pEnd, uint32_t events
             const float l = af_lo(*cc[j]), h = af_hi(*cc[j]);
             if (l > 0.0f || h < 0.0f) return kCull;
             resolved = resolved && __fsub_ru(h, l) < eps;
+            if (forms) {
+                float r = cc[j]->r;
+#pragma unroll
+                for (int i = 0; i < N - 1; i++) r = __fadd_ru(r, fabsf(cc[j]->x[i]));
+                forms[k].c[j] = cc[j]->c;
+                forms[k].rad[j] = r;
+                forms[k].xe[j] = cc[j]->x[N - 1];
+            }
         }
+        if (forms) forms[k].valid = true;
     }
     return resolved ? kLeaf : kSplit;
+}
+
+// eta^2 - 1 over the bins as an affine form: centre + radius * (its own noise symbol)
+template <int M> PZ_D Af<M> em1_form(float mLo, float mHi)
+{
+    Af<M> e = af_const<M>(__fmul_rn(__fadd_rn(mLo, mHi), 0.5f));
+    e.x[M - 1] = fmaxf(__fsub_ru(mHi, e.c), __fsub_ru(e.c, mLo));
+    return e;
+}
+
+// Can a root for bin value m of eta^2 - 1 lie in the box?  Substitutes the bin's value of
+// the eta symbol, (m - centre) / radius as an interval, into every vertex's residual
+// components; false when some component's range then excludes zero.
+template <int K>
+PZ_D bool bin_may_hold_root(const VertexForms* forms, const Af<2 * K + 1>& em1, float m)
+{
+    constexpr int M = 2 * K + 1;
+    const float rad = em1.x[M - 1];
+    float elo = 0.0f, ehi = 0.0f;
+    if (rad > 0.0f) {
+        elo = __fdiv_rd(__fsub_rd(m, em1.c), rad);
+        ehi = __fdiv_ru(__fsub_ru(m, em1.c), rad);
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        if (!forms[k].valid) continue;
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const float xe = forms[k].xe[j];
+            const float pl = fminf(__fmul_rd(xe, elo), __fmul_rd(xe, ehi));
+            const float ph = fmaxf(__fmul_ru(xe, elo), __fmul_ru(xe, ehi));
+            const float l = __fsub_rd(__fadd_rd(forms[k].c[j], pl), forms[k].rad[j]);
+            const float h = __fadd_ru(__fadd_ru(forms[k].c[j], ph), forms[k].rad[j]);
+            if (l > 0.0f || h < 0.0f) return false;
+        }
+    }
+    return true;
 }
 
 // ---------------------------------------------------------------- kernels
@@ -341,6 +403,9 @@ struct SubArgs {
     float* em1;         // [2]: range of eta^2 - 1 over the bins
     uint64_t* leaves;
     unsigned long long* nLeaves;
+    uint64_t* items;  // (leaf, bin) pairs to solve, in the two frontiers' space
+    unsigned long long* nItems;
+    uint64_t itemCapacity;
     pz_specular_root* roots;
     unsigned long long* nRoots;
     uint64_t rootCapacity;
@@ -409,10 +474,7 @@ __global__ void __launch_bounds__(kBlock) k_sub_round(SubArgs a, int depth, cons
 {
     constexpr int N = 2 * K;
     const uint64_t nIn = min((uint64_t)*countIn, a.capacity);
-    // eta^2 - 1 over the bins: centre and radius, rounded outward
-    const float mLo = a.em1[0], mHi = a.em1[1];
-    Af<N> em1 = af_const<N>(__fmul_rn(__fadd_rn(mLo, mHi), 0.5f));
-    em1.r = fmaxf(__fsub_ru(mHi, em1.c), __fsub_ru(em1.c, mLo));
+    const Af<N + 1> em1 = em1_form<N + 1>(a.em1[0], a.em1[1]);
     const bool last = depth >= a.maxDepth;
     for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nIn; e += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t ent = frontIn[e];
@@ -463,16 +525,52 @@ __device__ __noinline__ void polish_root(float* xs, const Chain<K>& ch, float3 p
     }
 }
 
+// One thread per leaf: the box's residual forms once, then for every bin the test of
+// bin_may_hold_root; the (leaf, bin) pairs that pass go to the solve list (leaf << 8 | bin).
 template <int K>
-__global__ void __launch_bounds__(kBlock) k_sub_leaves(SubArgs a)
+__global__ void __launch_bounds__(kBlock) k_sub_leaf_test(SubArgs a)
 {
     constexpr int N = 2 * K;
-    const uint64_t nItems = min((uint64_t)*a.nLeaves, a.capacity) * a.nBins;
+    const uint64_t nLeaves = min((uint64_t)*a.nLeaves, a.capacity);
+    const Af<N + 1> em1 = em1_form<N + 1>(a.em1[0], a.em1[1]);
+    for (uint64_t li = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; li < nLeaves;
+         li += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t ent = a.leaves[li];
+        const uint32_t row = (uint32_t)(ent >> 32), path = (uint32_t)ent & kPathMask;
+        const int depth = (int)(((uint32_t)ent >> kMaxDepth) & 31u);
+        Chain<K> ch;
+        uint32_t q;
+        load_row<K>(ch, a, row, &q);
+        float lo[N], hi[N];
+        box_bounds<N>(path, depth, lo, hi);
+        VertexForms forms[K];
+        const bool live = bound_box<K>(ch, a.pBeg, a.pEnd[q], a.events, em1, lo, hi, a.eps, forms) != kCull;
+        for (uint32_t b = 0; b < a.nBins; b++) {
+            const float e = a.etas[b];
+            const bool pass = live && bin_may_hold_root<K>(forms, em1, __fsub_rn(__fmul_rn(e, e), 1.0f));
+            if (a.stats) warp_count(a.stats + kStExcluded, !pass);
+            const unsigned long long s = warp_append(a.nItems, pass);
+            if (pass) {
+                if (s < a.itemCapacity) a.items[s] = (li << 8) | b;
+                else raise_error(a.status, kErrCapacity);
+            }
+        }
+    }
+}
+
+// One thread per (leaf, bin) pair of the solve list: Newton from the box centre,
+// ownership, throughput, root output.
+template <int K>
+__global__ void __launch_bounds__(kBlock) k_sub_leaf_solve(SubArgs a)
+{
+    constexpr int N = 2 * K;
+    const uint64_t nItems = min((uint64_t)*a.nItems, a.itemCapacity);
     const uint32_t root = __ldg(a.root);
     for (uint64_t it = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; it < nItems;
          it += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t ent = a.leaves[it / a.nBins];
-        const uint32_t bin = (uint32_t)(it % a.nBins);
+        const uint64_t item = a.items[it];
+        const uint64_t ent = a.leaves[item >> 8];
+        const uint32_t bin = (uint32_t)(item & 0xFFu);
         const uint32_t row = (uint32_t)(ent >> 32), path = (uint32_t)ent & kPathMask;
         const int depth = (int)(((uint32_t)ent >> kMaxDepth) & 31u);
         Chain<K> ch;
@@ -587,7 +685,10 @@ static cudaError_t run(SubArgs& a, uint64_t* fronts[2], unsigned long long* coun
         cur ^= 1;
     }
     if (e != cudaSuccess) return e;
-    k_sub_leaves<K><<<grid * 2, kBlock, 0, s>>>(a);
+    k_sub_leaf_test<K><<<grid, kBlock, 0, s>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_sub_leaf_solve<K><<<grid * 2, kBlock, 0, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -598,10 +699,10 @@ using namespace pz;
 using namespace pz::subdiv;
 
 static_assert(sizeof(pz_specular_root) == 64, "pz_specular_root layout");
-static_assert(kNumStats <= 8, "stats fit the header");
+static_assert(56 + 8 * kNumStats <= 256, "stats fit the header");
 
 namespace {
-constexpr size_t kHeader = 256;  // status | em1[2] | counts[2] | leaf count | root count | stats[7]
+constexpr size_t kHeader = 256;  // status | em1[2] | counts[2] | leaf, root, item counts | stats
 }
 
 extern "C" size_t pz_subdivide_scratch_bytes(uint64_t box_capacity)
@@ -649,7 +750,8 @@ extern "C" int pz_subdivide_solve(int K, uint32_t events, pz_float3 p_beg, const
     unsigned long long* counts = reinterpret_cast<unsigned long long*>(base + 16);  // [2]
     unsigned long long* nLeaves = reinterpret_cast<unsigned long long*>(base + 32);
     unsigned long long* nRoots = reinterpret_cast<unsigned long long*>(base + 40);
-    unsigned long long* stats = reinterpret_cast<unsigned long long*>(base + 48);  // [kNumStats]
+    unsigned long long* nItems = reinterpret_cast<unsigned long long*>(base + 48);
+    unsigned long long* stats = reinterpret_cast<unsigned long long*>(base + 56);  // [kNumStats]
     uint64_t* fronts[2] = {reinterpret_cast<uint64_t*>(base + kHeader),
                            reinterpret_cast<uint64_t*>(base + kHeader + part)};
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -677,6 +779,9 @@ extern "C" int pz_subdivide_solve(int K, uint32_t events, pz_float3 p_beg, const
     a.em1 = em1;
     a.leaves = reinterpret_cast<uint64_t*>(base + kHeader + 2 * part);
     a.nLeaves = nLeaves;
+    a.items = fronts[0];  // the frontiers are free once the rounds are done
+    a.nItems = nItems;
+    a.itemCapacity = 2 * a.capacity;
     a.roots = roots_dev;
     a.nRoots = nRoots;
     a.rootCapacity = root_capacity;
@@ -693,24 +798,25 @@ extern "C" int pz_subdivide_solve(int K, uint32_t events, pz_float3 p_beg, const
         }
     }
     if (e != cudaSuccess) return cuda_fail(e, "pz_subdivide_solve: launch");
-    unsigned long long hdr[6 + kNumStats];
+    unsigned long long hdr[7 + kNumStats];
     e = cudaMemcpyAsync(hdr, base, sizeof(hdr), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(e, "pz_subdivide_solve: results");
     const uint32_t st = (uint32_t)(hdr[0] & 0xFFFFFFFFull);
     *n_roots_out = hdr[5];
     if (stats_out) {
-        stats_out->boxes_tested = hdr[6 + kStTested];
-        stats_out->boxes_culled = hdr[6 + kStCulled];
+        stats_out->boxes_tested = hdr[7 + kStTested];
+        stats_out->boxes_culled = hdr[7 + kStCulled];
         stats_out->leaves = hdr[4];
-        stats_out->solves = hdr[6 + kStSolves];
-        stats_out->converged = hdr[6 + kStConverged];
-        stats_out->outside_box = hdr[6 + kStOutside];
-        stats_out->roots = hdr[6 + kStRoots];
-        stats_out->polished = hdr[6 + kStPolished];
+        stats_out->bins_excluded = hdr[7 + kStExcluded];
+        stats_out->solves = hdr[7 + kStSolves];
+        stats_out->converged = hdr[7 + kStConverged];
+        stats_out->outside_box = hdr[7 + kStOutside];
+        stats_out->roots = hdr[7 + kStRoots];
+        stats_out->polished = hdr[7 + kStPolished];
     }
     if (st & kErrCapacity)
-        return fail(PZ_ERR_DEVICE, "pz_subdivide_solve: capacity exceeded (%llu roots for %llu slots, or the box lists)",
+        return fail(PZ_ERR_DEVICE, "pz_subdivide_solve: capacity exceeded (%llu roots for %llu slots, or the box / solve lists)",
                     (unsigned long long)hdr[5], (unsigned long long)root_capacity);
     clear_error();
     return PZ_OK;

@@ -213,11 +213,13 @@ def test_live_render_vs_reference(orc, ref):
 
 def test_subdivision_finds_every_root_of_dense_starts(orc):
     """The subdivision solve (pz_oracle_subdiv.hpp, the checker of pz_subdivide_solve) has no
-    reference counterpart; it is pinned by a property: every contributing root that the
-    reference's Newton solve (solveConstraints<K>, pk.h:466-592) reaches from a dense grid
-    of starts in any (receiver point, lens triangle) domain is among its roots, and it
-    reports no root the grid does not find (within 1e-3 in the barycentrics: roots of
-    ill-conditioned tuples stop anywhere in a 1e-4-wide basin)."""
+    reference counterpart; it is pinned by a property: for every wavelength bin, every
+    contributing root that the reference's Newton solve (solveConstraints<K>,
+    pk.h:466-592) reaches from a dense grid of starts in any (receiver point, lens
+    triangle) domain is among its roots, and it reports no root the grid does not find
+    (within 1e-3 in the barycentrics: roots of ill-conditioned tuples stop anywhere in a
+    1e-4-wide basin).  Three bins share the subdivision, so the per-bin leaf test is
+    covered too."""
     sc = S.lens_scene(side=8, seed=5, amplitude=0.05, events="T", width=16, height=16)
     ev = S.event_descriptor("T")
     bvh = orc.build_bvh(sc.tris, 0)
@@ -226,26 +228,27 @@ def test_subdivision_finds_every_root_of_dense_starts(orc):
     ends[:, 1] = 0.0
     spec = np.nonzero(sc.attribs["material"] != 0)[0]
     rows = np.array([[q, i] for q in range(len(ends)) for i in spec], np.uint32)
-    roots, stats = orc.subdivide_solve(1, ev, sc.p_light, ends, rows, np.array([1.5], np.float32), sc.tris, sc.attribs,
-                                       bvh, sc.tris)
-    assert stats[1] > len(rows) // 2 and len(roots) > 10
+    etas = np.array([1.5, 1.53, 1.56], np.float32)
+    roots, stats = orc.subdivide_solve(1, ev, sc.p_light, ends, rows, etas, sc.tris, sc.attribs, bvh, sc.tris)
+    assert stats[1] > len(rows) // 2 and stats[3] > 0 and len(roots) > 30
     sub = {}
     for r in roots:
-        sub.setdefault(int(r["tuple"]), []).append(r["params"][:2])
+        sub.setdefault((int(r["tuple"]), int(r["bin"])), []).append(r["params"][:2])
     grid = [(u, v) for u in np.linspace(0.02, 0.98, 9) for v in np.linspace(0.02, 0.98, 9) if u + v <= 1.0]
     brute = {}
     for ri, (q, tri) in enumerate(rows):
         T, At = sc.tris[[tri]], sc.attribs[[tri]]
-        for u, v in grid:
-            ok, p, _ = orc.solve_constraints(1, np.array([u, v], np.float32), sc.p_light, ends[q], T, At, 1.5, ev)
-            if ok and orc.contributable_throughput(1, p, sc.p_light, ends[q], T, At, ev, bvh, sc.tris, 1.5) > 0:
-                lst = brute.setdefault(ri, [])
-                if not any(np.abs(p - x).max() < 1e-4 for x in lst):
-                    lst.append(p)
-    for ri in set(sub) | set(brute):
-        a, b = sub.get(ri, []), brute.get(ri, [])
-        assert all(any(np.abs(p - x).max() < 1e-3 for x in a) for p in b), ri
-        assert all(any(np.abs(p - x).max() < 1e-3 for p in b) for x in a), ri
+        for b, eta in enumerate(etas):
+            for u, v in grid:
+                ok, p, _ = orc.solve_constraints(1, np.array([u, v], np.float32), sc.p_light, ends[q], T, At, eta, ev)
+                if ok and orc.contributable_throughput(1, p, sc.p_light, ends[q], T, At, ev, bvh, sc.tris, eta) > 0:
+                    lst = brute.setdefault((ri, b), [])
+                    if not any(np.abs(p - x).max() < 1e-4 for x in lst):
+                        lst.append(p)
+    for key in set(sub) | set(brute):
+        a, b = sub.get(key, []), brute.get(key, [])
+        assert all(any(np.abs(p - x).max() < 1e-3 for x in a) for p in b), key
+        assert all(any(np.abs(p - x).max() < 1e-3 for p in b) for x in a), key
 
 
 def _f32_neighbours(x):

@@ -49,7 +49,7 @@ def _check_equal(exp, ids, params, thr, K):
     assert thr.tobytes() == exp["throughput"].tobytes()
 
 
-STAT_KEYS = ("boxes_tested", "boxes_culled", "leaves", "solves", "converged", "outside_box", "roots")
+STAT_KEYS = ("boxes_tested", "boxes_culled", "leaves", "bins_excluded", "solves", "converged", "outside_box", "roots")
 
 
 @pytest.mark.parametrize("amplitude,side,bins", [(0.01, 32, 1), (0.03, 16, 1), (0.05, 8, 4)])
