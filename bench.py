@@ -608,6 +608,7 @@ def run_subdivision(args):
     ms_plain = e0.elapsed_time(e1) / args.steps
     cpu = None
     if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as O
         orc = O.oracle()
         bo = orc.build_bvh(sc.tris, 0)
