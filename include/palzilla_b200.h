@@ -349,7 +349,8 @@ typedef struct pz_specular_root {
 PZ_API size_t pz_subdivide_scratch_bytes(uint64_t box_capacity);
 /* Writes the kept roots (unordered) to roots_dev and their count (which may exceed
  * root_capacity: PZ_ERR_DEVICE is then returned) to *n_roots_out.  Synchronises `stream`
- * once, at the end. */
+ * twice: for the leaf count (the leaves are sorted by tuple row before they are solved)
+ * and at the end. */
 PZ_API int pz_subdivide_solve(int K, uint32_t events, pz_float3 p_beg, const pz_float3* p_end_dev,
                               const uint32_t* tuples_dev, uint32_t n_tuples, const float* etas_dev, int n_bins,
                               const pz_subdiv_params* params, const pz_triangle* triangles_dev,

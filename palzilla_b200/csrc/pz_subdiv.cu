@@ -670,8 +670,30 @@ __global__ void __launch_bounds__(kBlock) k_sub_contribute(ContribArgs a)
     }
 }
 
+// Sorts the leaf list by tuple row (a stable onesweep sort on the entries' upper 32 bits,
+// the frontiers as ping-pong buffer and sort scratch) so that the leaf kernels see the
+// rows -- and their triangles and visibility rays -- in the work list's coherent order.
+// The set of roots does not depend on the order.  Reads the leaf count back (one
+// synchronisation); skipped for small lists or when the frontier cannot hold the sort's
+// scratch.
+static cudaError_t sort_leaves(const SubArgs& a, uint64_t* fronts[2], size_t part, cudaStream_t s)
+{
+    unsigned long long nl = 0;
+    cudaError_t e = cudaMemcpyAsync(&nl, a.nLeaves, sizeof(nl), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    nl = std::min<unsigned long long>(nl, a.capacity);
+    if (nl <= 4096 || part < pz_onesweep_scratch_bytes((uint32_t)nl)) return cudaSuccess;
+    const int bits = a.nRows > 1 ? 32 - __builtin_clz(a.nRows - 1) : 1;
+    const int endBit = 32 + 8 * ((bits + 7) / 8);
+    if (pz_onesweep_sort(a.leaves, nullptr, fronts[0], nullptr, (uint32_t)nl, 8, 32, endBit, fronts[1], part,
+                         reinterpret_cast<pz_stream_t>(s)) != PZ_OK)
+        return cudaErrorUnknown;
+    return cudaSuccess;
+}
+
 template <int K>
-static cudaError_t run(SubArgs& a, uint64_t* fronts[2], unsigned long long* counts, cudaStream_t s)
+static cudaError_t run(SubArgs& a, uint64_t* fronts[2], size_t part, unsigned long long* counts, cudaStream_t s)
 {
     const int grid = kNumSMs * 8;
     k_sub_init<<<(a.nRows + kBlock - 1) / kBlock, kBlock, 0, s>>>(a, fronts[0], &counts[0]);
@@ -684,6 +706,8 @@ static cudaError_t run(SubArgs& a, uint64_t* fronts[2], unsigned long long* coun
         e = cudaGetLastError();
         cur ^= 1;
     }
+    if (e != cudaSuccess) return e;
+    e = sort_leaves(a, fronts, part, s);
     if (e != cudaSuccess) return e;
     k_sub_leaf_test<K><<<grid, kBlock, 0, s>>>(a);
     e = cudaGetLastError();
@@ -791,10 +815,10 @@ extern "C" int pz_subdivide_solve(int K, uint32_t events, pz_float3 p_beg, const
     cudaError_t e = cudaMemsetAsync(base, 0, kHeader, s);
     if (e == cudaSuccess) {
         switch (K) {
-            case 1: e = run<1>(a, fronts, counts, s); break;
-            case 2: e = run<2>(a, fronts, counts, s); break;
-            case 3: e = run<3>(a, fronts, counts, s); break;
-            default: e = run<4>(a, fronts, counts, s); break;
+            case 1: e = run<1>(a, fronts, part, counts, s); break;
+            case 2: e = run<2>(a, fronts, part, counts, s); break;
+            case 3: e = run<3>(a, fronts, part, counts, s); break;
+            default: e = run<4>(a, fronts, part, counts, s); break;
         }
     }
     if (e != cudaSuccess) return cuda_fail(e, "pz_subdivide_solve: launch");
