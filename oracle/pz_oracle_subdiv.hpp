@@ -296,17 +296,21 @@ template <int M> Af<M> em1_form(float mLo, float mHi)
     return e;
 }
 
-// can a root for the bin value m of eta^2 - 1 lie in the box (the leaf test)?
-template <int K>
-bool bin_may_hold_root(const VertexForms* forms, const Af<2 * K + 1>& em1, float m)
+// the eta symbol's value for the bin value m of eta^2 - 1, as an interval
+template <int M> void bin_symbol(const Af<M>& em1, float m, float* elo, float* ehi)
 {
-    constexpr int M = 2 * K + 1;
     const float rad = em1.x[M - 1];
-    float elo = 0.0f, ehi = 0.0f;
+    *elo = *ehi = 0.0f;
     if (rad > 0.0f) {
-        elo = div_d(sub_d(m, em1.c), rad);
-        ehi = div_u(sub_u(m, em1.c), rad);
+        *elo = div_d(sub_d(m, em1.c), rad);
+        *ehi = div_u(sub_u(m, em1.c), rad);
     }
+}
+
+// can a root for a bin (eta symbol in [elo, ehi]) lie in the box (the leaf test)?
+template <int K>
+bool bin_may_hold_root(const VertexForms* forms, float elo, float ehi)
+{
     for (int k = 0; k < K; k++) {
         if (!forms[k].valid) continue;
         for (int j = 0; j < 3; j++) {
@@ -378,7 +382,9 @@ void solve_row(uint32_t row, const uint32_t* tuples, uint32_t events, F3 pBeg, c
         VertexForms forms[K];
         bound_box<K>(tris, attribs, pBeg, pEnd[q], events, em1, bl, bh, P.eps, forms);
         for (int b = 0; b < nBins; b++) {
-            if (!bin_may_hold_root<K>(forms, em1, etas[b] * etas[b] - 1.0f)) {
+            float elo, ehi;
+            bin_symbol(em1, etas[b] * etas[b] - 1.0f, &elo, &ehi);
+            if (!bin_may_hold_root<K>(forms, elo, ehi)) {
                 stats[3]++;
                 continue;
             }

@@ -350,19 +350,24 @@ template <int M> PZ_D Af<M> em1_form(float mLo, float mHi)
     return e;
 }
 
-// Can a root for bin value m of eta^2 - 1 lie in the box?  Substitutes the bin's value of
-// the eta symbol, (m - centre) / radius as an interval, into every vertex's residual
-// components; false when some component's range then excludes zero.
-template <int K>
-PZ_D bool bin_may_hold_root(const VertexForms* forms, const Af<2 * K + 1>& em1, float m)
+// The eta symbol's value for the bin value m of eta^2 - 1: (m - centre) / radius, as an
+// interval [*elo, *ehi].
+template <int M> PZ_D void bin_symbol(const Af<M>& em1, float m, float* elo, float* ehi)
 {
-    constexpr int M = 2 * K + 1;
     const float rad = em1.x[M - 1];
-    float elo = 0.0f, ehi = 0.0f;
+    *elo = *ehi = 0.0f;
     if (rad > 0.0f) {
-        elo = __fdiv_rd(__fsub_rd(m, em1.c), rad);
-        ehi = __fdiv_ru(__fsub_ru(m, em1.c), rad);
+        *elo = __fdiv_rd(__fsub_rd(m, em1.c), rad);
+        *ehi = __fdiv_ru(__fsub_ru(m, em1.c), rad);
     }
+}
+
+// Can a root for a bin lie in the box?  Substitutes the bin's value of the eta symbol,
+// [elo, ehi], into every vertex's residual components; false when some component's range
+// then excludes zero.
+template <int K>
+PZ_D bool bin_may_hold_root(const VertexForms* forms, float elo, float ehi)
+{
 #pragma unroll
     for (int k = 0; k < K; k++) {
         if (!forms[k].valid) continue;
@@ -531,8 +536,16 @@ template <int K>
 __global__ void __launch_bounds__(kBlock) k_sub_leaf_test(SubArgs a)
 {
     constexpr int N = 2 * K;
+    __shared__ float2 binSymbol[kMaxBins];
     const uint64_t nLeaves = min((uint64_t)*a.nLeaves, a.capacity);
     const Af<N + 1> em1 = em1_form<N + 1>(a.em1[0], a.em1[1]);
+    for (uint32_t b = threadIdx.x; b < a.nBins; b += blockDim.x) {
+        const float e = a.etas[b];
+        float lo, hi;
+        bin_symbol(em1, __fsub_rn(__fmul_rn(e, e), 1.0f), &lo, &hi);
+        binSymbol[b] = make_float2(lo, hi);
+    }
+    __syncthreads();
     for (uint64_t li = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; li < nLeaves;
          li += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t ent = a.leaves[li];
@@ -546,8 +559,8 @@ __global__ void __launch_bounds__(kBlock) k_sub_leaf_test(SubArgs a)
         VertexForms forms[K];
         const bool live = bound_box<K>(ch, a.pBeg, a.pEnd[q], a.events, em1, lo, hi, a.eps, forms) != kCull;
         for (uint32_t b = 0; b < a.nBins; b++) {
-            const float e = a.etas[b];
-            const bool pass = live && bin_may_hold_root<K>(forms, em1, __fsub_rn(__fmul_rn(e, e), 1.0f));
+            const float2 sym = binSymbol[b];
+            const bool pass = live && bin_may_hold_root<K>(forms, sym.x, sym.y);
             if (a.stats) warp_count(a.stats + kStExcluded, !pass);
             const unsigned long long s = warp_append(a.nItems, pass);
             if (pass) {
@@ -560,7 +573,7 @@ __global__ void __launch_bounds__(kBlock) k_sub_leaf_test(SubArgs a)
 
 // One thread per (leaf, bin) pair of the solve list: Newton from the box centre,
 // ownership, throughput, root output.
-template <int K>
+template <int K, bool kPolish>
 __global__ void __launch_bounds__(kBlock) k_sub_leaf_solve(SubArgs a)
 {
     constexpr int N = 2 * K;
@@ -589,7 +602,7 @@ __global__ void __launch_bounds__(kBlock) k_sub_leaf_solve(SubArgs a)
 #pragma unroll
         for (int j = 0; j < N; j++)
             inside = inside && lo[j] <= xs[j] && (xs[j] < hi[j] || (hi[j] == 1.0f && xs[j] == 1.0f));
-        if (inside && a.polish) polish_root<K>(xs, ch, a.pBeg, pEnd, a.events, eta);
+        if (kPolish && inside) polish_root<K>(xs, ch, a.pBeg, pEnd, a.events, eta);
         float thr = 0.0f;
         if (inside)
             thr = solver::contributable_throughput<float, K>(xs, solver::v3f<float>(a.pBeg), solver::v3f<float>(pEnd),
@@ -600,7 +613,7 @@ __global__ void __launch_bounds__(kBlock) k_sub_leaf_solve(SubArgs a)
             warp_count(a.stats + kStConverged, conv);
             warp_count(a.stats + kStOutside, conv && !inside);
             warp_count(a.stats + kStRoots, emit);
-            warp_count(a.stats + kStPolished, inside && a.polish);
+            warp_count(a.stats + kStPolished, kPolish && inside);
         }
         const unsigned long long s = warp_append(a.nRoots, emit);
         if (emit) {
@@ -712,7 +725,8 @@ static cudaError_t run(SubArgs& a, uint64_t* fronts[2], size_t part, unsigned lo
     k_sub_leaf_test<K><<<grid, kBlock, 0, s>>>(a);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_sub_leaf_solve<K><<<grid * 2, kBlock, 0, s>>>(a);
+    if (a.polish) k_sub_leaf_solve<K, true><<<grid * 2, kBlock, 0, s>>>(a);
+    else k_sub_leaf_solve<K, false><<<grid * 2, kBlock, 0, s>>>(a);
     return cudaGetLastError();
 }
 
