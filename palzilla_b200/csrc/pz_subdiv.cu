@@ -435,6 +435,45 @@ PZ_D unsigned long long warp_append(unsigned long long* counter, bool want)
     return base + __popc(ballot & ((1u << (threadIdx.x & 31)) - 1u));
 }
 
+// Sum of v over the active lanes (*total) and this lane's exclusive prefix of it, by one
+// shuffle per lane of the warp (correct for any set of active lanes).
+PZ_D uint32_t warp_prefix(uint32_t active, uint32_t v, uint32_t* total)
+{
+    const int lane = (int)(threadIdx.x & 31);
+    uint32_t pre = 0, tot = 0;
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+        const uint32_t x = __shfl_sync(active, v, j);
+        if ((active >> j) & 1u) {
+            tot += x;
+            if (j < lane) pre += x;
+        }
+    }
+    *total = tot;
+    return pre;
+}
+
+// warp-aggregated reservation of n consecutive slots per lane: one atomic per warp
+PZ_D unsigned long long warp_reserve(unsigned long long* counter, uint32_t n)
+{
+    const uint32_t active = __activemask();
+    const int leader = __ffs(active) - 1;
+    uint32_t total;
+    const uint32_t pre = warp_prefix(active, n, &total);
+    unsigned long long base = 0;
+    if ((int)(threadIdx.x & 31) == leader && total) base = atomicAdd(counter, (unsigned long long)total);
+    base = __shfl_sync(active, base, leader);
+    return base + pre;
+}
+
+PZ_D void warp_sum(unsigned long long* stat, uint32_t v)
+{
+    const uint32_t active = __activemask();
+    uint32_t total;
+    warp_prefix(active, v, &total);
+    if ((int)(threadIdx.x & 31) == __ffs(active) - 1 && total) atomicAdd(stat, (unsigned long long)total);
+}
+
 PZ_D void warp_count(unsigned long long* stat, bool v)
 {
     const uint32_t active = __activemask();
@@ -558,14 +597,30 @@ __global__ void __launch_bounds__(kBlock) k_sub_leaf_test(SubArgs a)
         box_bounds<N>(path, depth, lo, hi);
         VertexForms forms[K];
         const bool live = bound_box<K>(ch, a.pBeg, a.pEnd[q], a.events, em1, lo, hi, a.eps, forms) != kCull;
-        for (uint32_t b = 0; b < a.nBins; b++) {
-            const float2 sym = binSymbol[b];
-            const bool pass = live && bin_may_hold_root<K>(forms, sym.x, sym.y);
-            if (a.stats) warp_count(a.stats + kStExcluded, !pass);
-            const unsigned long long s = warp_append(a.nItems, pass);
-            if (pass) {
-                if (s < a.itemCapacity) a.items[s] = (li << 8) | b;
+        if (a.nBins <= 64) {
+            // the passing bins as a mask, then one warp-wide append for all of them
+            uint64_t mask = 0;
+            for (uint32_t b = 0; b < a.nBins; b++) {
+                const float2 sym = binSymbol[b];
+                if (live && bin_may_hold_root<K>(forms, sym.x, sym.y)) mask |= 1ull << b;
+            }
+            const uint32_t cnt = (uint32_t)__popcll(mask);
+            if (a.stats) warp_sum(a.stats + kStExcluded, a.nBins - cnt);
+            unsigned long long slot = warp_reserve(a.nItems, cnt);
+            for (; mask; mask &= mask - 1, slot++) {
+                if (slot < a.itemCapacity) a.items[slot] = (li << 8) | (uint64_t)__ffsll((long long)mask) - 1;
                 else raise_error(a.status, kErrCapacity);
+            }
+        } else {
+            for (uint32_t b = 0; b < a.nBins; b++) {
+                const float2 sym = binSymbol[b];
+                const bool pass = live && bin_may_hold_root<K>(forms, sym.x, sym.y);
+                if (a.stats) warp_count(a.stats + kStExcluded, !pass);
+                const unsigned long long s = warp_append(a.nItems, pass);
+                if (pass) {
+                    if (s < a.itemCapacity) a.items[s] = (li << 8) | b;
+                    else raise_error(a.status, kErrCapacity);
+                }
             }
         }
     }
