@@ -474,13 +474,6 @@ PZ_D void warp_sum(unsigned long long* stat, uint32_t v)
     if ((int)(threadIdx.x & 31) == __ffs(active) - 1 && total) atomicAdd(stat, (unsigned long long)total);
 }
 
-PZ_D void warp_count(unsigned long long* stat, bool v)
-{
-    const uint32_t active = __activemask();
-    const uint32_t b = __ballot_sync(active, v);
-    if ((int)(threadIdx.x & 31) == __ffs(active) - 1 && b) atomicAdd(stat, (unsigned long long)__popc(b));
-}
-
 template <int K>
 PZ_D void load_row(Chain<K>& ch, const SubArgs& a, uint32_t row, uint32_t* q)
 {
@@ -520,6 +513,7 @@ __global__ void __launch_bounds__(kBlock) k_sub_round(SubArgs a, int depth, cons
     const uint64_t nIn = min((uint64_t)*countIn, a.capacity);
     const Af<N + 1> em1 = em1_form<N + 1>(a.em1[0], a.em1[1]);
     const bool last = depth >= a.maxDepth;
+    uint32_t tested = 0, culled = 0;
     for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nIn; e += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t ent = frontIn[e];
         const uint32_t row = (uint32_t)(ent >> 32), path = (uint32_t)ent & kPathMask;
@@ -530,23 +524,26 @@ __global__ void __launch_bounds__(kBlock) k_sub_round(SubArgs a, int depth, cons
         box_bounds<N>(path, depth, lo, hi);
         int v = bound_box<K>(ch, a.pBeg, a.pEnd[q], a.events, em1, lo, hi, a.eps);
         if (v == kSplit && last) v = kLeaf;
-        if (a.stats) {
-            warp_count(a.stats + kStTested, true);
-            warp_count(a.stats + kStCulled, v == kCull);
-        }
+        tested++;
+        culled += v == kCull;
         const unsigned long long ls = warp_append(a.nLeaves, v == kLeaf);
         if (v == kLeaf) {
             if (ls < a.capacity) a.leaves[ls] = make_entry(row, depth, path);
             else raise_error(a.status, kErrCapacity);
         }
-        const bool split = v == kSplit;
-        for (uint32_t half = 0; half < 2; half++) {
-            const unsigned long long s = warp_append(countOut, split);
-            if (split) {
-                if (s < a.capacity) frontOut[s] = make_entry(row, depth + 1, path | (half << depth));
-                else raise_error(a.status, kErrCapacity);
+        const unsigned long long s = warp_reserve(countOut, v == kSplit ? 2u : 0u);
+        if (v == kSplit) {
+            if (s + 1 < a.capacity) {
+                frontOut[s] = make_entry(row, depth + 1, path);
+                frontOut[s + 1] = make_entry(row, depth + 1, path | (1u << depth));
+            } else {
+                raise_error(a.status, kErrCapacity);
             }
         }
+    }
+    if (a.stats) {
+        warp_sum(a.stats + kStTested, tested);
+        warp_sum(a.stats + kStCulled, culled);
     }
 }
 
@@ -585,6 +582,7 @@ __global__ void __launch_bounds__(kBlock) k_sub_leaf_test(SubArgs a)
         binSymbol[b] = make_float2(lo, hi);
     }
     __syncthreads();
+    uint32_t excluded = 0;
     for (uint64_t li = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; li < nLeaves;
          li += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t ent = a.leaves[li];
@@ -605,7 +603,7 @@ __global__ void __launch_bounds__(kBlock) k_sub_leaf_test(SubArgs a)
                 if (live && bin_may_hold_root<K>(forms, sym.x, sym.y)) mask |= 1ull << b;
             }
             const uint32_t cnt = (uint32_t)__popcll(mask);
-            if (a.stats) warp_sum(a.stats + kStExcluded, a.nBins - cnt);
+            excluded += a.nBins - cnt;
             unsigned long long slot = warp_reserve(a.nItems, cnt);
             for (; mask; mask &= mask - 1, slot++) {
                 if (slot < a.itemCapacity) a.items[slot] = (li << 8) | (uint64_t)__ffsll((long long)mask) - 1;
@@ -615,7 +613,7 @@ __global__ void __launch_bounds__(kBlock) k_sub_leaf_test(SubArgs a)
             for (uint32_t b = 0; b < a.nBins; b++) {
                 const float2 sym = binSymbol[b];
                 const bool pass = live && bin_may_hold_root<K>(forms, sym.x, sym.y);
-                if (a.stats) warp_count(a.stats + kStExcluded, !pass);
+                excluded += !pass;
                 const unsigned long long s = warp_append(a.nItems, pass);
                 if (pass) {
                     if (s < a.itemCapacity) a.items[s] = (li << 8) | b;
@@ -624,6 +622,7 @@ __global__ void __launch_bounds__(kBlock) k_sub_leaf_test(SubArgs a)
             }
         }
     }
+    if (a.stats) warp_sum(a.stats + kStExcluded, excluded);
 }
 
 // One thread per (leaf, bin) pair of the solve list: Newton from the box centre,
@@ -634,6 +633,7 @@ __global__ void __launch_bounds__(kBlock) k_sub_leaf_solve(SubArgs a)
     constexpr int N = 2 * K;
     const uint64_t nItems = min((uint64_t)*a.nItems, a.itemCapacity);
     const uint32_t root = __ldg(a.root);
+    uint32_t nSolves = 0, nConverged = 0, nOutside = 0, nRoots = 0;
     for (uint64_t it = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; it < nItems;
          it += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t item = a.items[it];
@@ -663,13 +663,10 @@ __global__ void __launch_bounds__(kBlock) k_sub_leaf_solve(SubArgs a)
             thr = solver::contributable_throughput<float, K>(xs, solver::v3f<float>(a.pBeg), solver::v3f<float>(pEnd),
                                                              ch, a.events, a.nodes, a.sceneTris, root, eta);
         const bool emit = thr > 0.0f;
-        if (a.stats) {
-            warp_count(a.stats + kStSolves, true);
-            warp_count(a.stats + kStConverged, conv);
-            warp_count(a.stats + kStOutside, conv && !inside);
-            warp_count(a.stats + kStRoots, emit);
-            warp_count(a.stats + kStPolished, kPolish && inside);
-        }
+        nSolves++;
+        nConverged += conv;
+        nOutside += conv && !inside;
+        nRoots += emit;
         const unsigned long long s = warp_append(a.nRoots, emit);
         if (emit) {
             if (s < a.rootCapacity) {
@@ -687,6 +684,13 @@ __global__ void __launch_bounds__(kBlock) k_sub_leaf_solve(SubArgs a)
                 raise_error(a.status, kErrCapacity);
             }
         }
+    }
+    if (a.stats) {
+        warp_sum(a.stats + kStSolves, nSolves);
+        warp_sum(a.stats + kStConverged, nConverged);
+        warp_sum(a.stats + kStOutside, nOutside);
+        warp_sum(a.stats + kStRoots, nRoots);
+        if (kPolish) warp_sum(a.stats + kStPolished, nConverged - nOutside);
     }
 }
 
