@@ -269,6 +269,23 @@ def lens_scene(side: int = 64, seed: int = 1, amplitude: float = 0.01, events: s
                  width=width, height=height)
 
 
+def stacked_lens_scene(sheets: int = 4, side: int = 24, seed: int = 1, amplitude: float = 0.01, n_bins: int = 8,
+                       width: int = 96, height: int = 96) -> Scene:
+    """Two heightfield lenses stacked over the receiver, for chains of 3 and 4 refractions:
+    a heightfield sheet at y=1 with a flat bottom at y=0.92, then a second heightfield
+    sheet (seed + 1) at y=0.80 with a flat bottom at y=0.72; `sheets` of these four
+    surfaces, from the top, are kept (events "T" * sheets).  The camera looks down from
+    y=0.6, below the glass."""
+    surf = [heightfield_lens(side, seed, amplitude), flat_sheet(16, 0.92),
+            heightfield_lens(side, seed + 1, amplitude, y=0.80), flat_sheet(16, 0.72)][:sheets]
+    tris, att = _combine(surf + [receiver_plane(1.0, 0.0)])
+    eye_y = 0.6
+    cam = Camera(eye=(0.0, eye_y, 0.0), center=(0.0, 0.0, 0.0), up=(0.0, 0.0, -1.0),
+                 fovy=2.0 * math.atan(0.5 / eye_y))
+    return Scene(name=f"stacked{sheets}", tris=tris, attribs=att, camera=cam, events="T" * sheets, n_bins=n_bins,
+                 width=width, height=height)
+
+
 def adjoint_scene(side: int = 128, seed: int = 1, width: int = 512, height: int = 512, n_bins: int = 8,
                   amplitude: float = 0.01):
     """Heightfield lens for gradient checks: the lens_scene with a side x side grid (the
