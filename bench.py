@@ -709,8 +709,8 @@ def _sample(pairs, n, seed):
 
 
 def cpu_baseline(R, seconds=15.0):
-    """The reference's CPU solve over a bounded sample of this frame's work items, OpenMP
-    over all host threads; about `seconds` of CPU work."""
+    """The reference's CPU solve over a bounded sample of this frame's work items (with the
+    frame's light point), OpenMP over all host threads; about `seconds` of CPU work."""
     lib, kind = _cpu_lib()
     import oracle as O
     sc = R.sc
@@ -723,12 +723,12 @@ def cpu_baseline(R, seconds=15.0):
     etas = sc.bin_etas()
     probe = _sample(pairs, 512, 1)
     t0 = time.perf_counter()
-    lib.render_pairs(2, probe, cache, fd, bvh, sc, etas)
+    lib.render_pairs(2, probe, cache, fd, bvh, sc, etas, iteration=R.iteration)
     dt = time.perf_counter() - t0
     m = int(min(len(pairs), max(512, len(probe) * seconds / max(dt, 1e-3))))
     sel = _sample(pairs, m, 2)
     t0 = time.perf_counter()
-    _, st = lib.render_pairs(2, sel, cache, fd, bvh, sc, etas)
+    _, st = lib.render_pairs(2, sel, cache, fd, bvh, sc, etas, iteration=R.iteration)
     dt = time.perf_counter() - t0
     return {"value": float(st[0]) / dt, "unit": UNIT, "cores": lib.max_threads(), "kind": kind,
             "sample": f"solve stage only: {len(sel)} of the frame's {n} (pixel, tuple) work items x 64 bins "
