@@ -501,8 +501,9 @@ def run_uneven_batch(args):
 def run_pathcuts(args):
     """Path Cuts (traverseAdmissibleNodes<2>, TT) on the two-sheet heightfield lens (side 64:
     8,388 triangles, USE_NORMAL BVH): admissible tuples of 4,096 receiver points on a grid,
-    round-to-nearest and directed rounding; the reference's CPU traversal (oracle/_ref) is
-    timed on a bounded sample of the points (one OpenMP thread per query)."""
+    round-to-nearest and directed rounding; the subdivision solve of the tuples of the first
+    256 points; the reference's CPU traversal (oracle/_ref) is timed on a bounded sample of
+    the points (one OpenMP thread per query)."""
     import torch
     from palzilla_b200 import api as A
     from palzilla_b200 import scenes as S
@@ -531,6 +532,23 @@ def run_pathcuts(args):
         ms = (time.perf_counter() - t0) * 1e3 / args.steps
         res[mode] = {"ms": ms, "tuples": int(rows.shape[0]), "node_tuples": int(visited),
                      "node_tuples_per_s": visited / (ms / 1e3), "queries_per_s": len(ends) / (ms / 1e3)}
+    # every root of the admissible tuples of the first 256 receiver points: the subdivision
+    # solve on the round-to-nearest Path Cuts rows (one bin, eta 1.52; the visibility BVH is
+    # the same tree, any BVH over the triangles answers the same any-hit queries)
+    sub_q = 256
+    rows_q, _ = pc.run(2, ev, 1.52, sc.p_light, ends_d[:sub_q], b, nbs, t, at)
+    solver = A.SubdivisionSolver(box_capacity=1 << 26, root_capacity=1 << 22)
+    eta1 = torch.tensor([1.52], device="cuda")
+    for i in range(args.warmup):
+        solver.run(2, ev, sc.p_light, ends_d, rows_q, eta1, t, at, b, t)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        _, _, _, sst = solver.run(2, ev, sc.p_light, ends_d, rows_q, eta1, t, at, b, t)
+    torch.cuda.synchronize()
+    sub_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    subdivision = {"queries": sub_q, "rows": int(rows_q.shape[0]), "ms": sub_ms, "stats": sst,
+                   "rows_per_s": int(rows_q.shape[0]) / (sub_ms / 1e3)}
     cpu = None
     lib, kind = _cpu_lib()
     if lib.has("path_cuts"):
@@ -548,7 +566,8 @@ def run_pathcuts(args):
     print(json.dumps({"metric": "Path Cuts queries/s (admissible K=2 tuples per receiver point)",
                       "workload": "pathcuts", "value": res["rn"]["queries_per_s"], "unit": "queries/s",
                       "higher_is_better": True, "data": "synthetic", "triangles": sc.n, "queries": len(ends),
-                      "round_to_nearest": res["rn"], "directed_rounding": res["dr"], "cpu_baseline": cpu}),
+                      "round_to_nearest": res["rn"], "directed_rounding": res["dr"],
+                      "subdivision_of_the_tuples": subdivision, "cpu_baseline": cpu}),
           flush=True)
 
 

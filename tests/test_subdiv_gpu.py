@@ -200,3 +200,28 @@ def test_host_checks():
                                 C.byref(n), None, None, 0, None) == 0 and n.value == 0
     assert L.pz_subdivide_contribute(1, 1, z, 1.0, 1.0, None, None, 0, None, None, 1, None, None, None, None) == 0
     assert L.pz_subdivide_scratch_bytes(1000) >= 256 + 3 * 8000
+
+
+def test_capacity_overflow_is_reported():
+    """A root list or box list too small for the work is reported as PZ_ERR_DEVICE (the
+    kernels drop what does not fit and set the capacity bit), and the counts still say how
+    many roots there were."""
+    sc = S.lens_scene(side=8, seed=5, amplitude=0.05, events="T", width=16, height=16)
+    t, at, b = _dev(sc)
+    ends = torch.from_numpy(_ends(6, 2)).cuda()
+    spec = np.nonzero(sc.attribs["material"] != 0)[0]
+    rows = torch.from_numpy(np.array([[q, i] for q in range(6) for i in spec], np.int32)).cuda()
+    etas = torch.tensor([1.5, 1.53, 1.56], device="cuda")
+    ev = S.event_descriptor("T")
+    ok = A.SubdivisionSolver(box_capacity=1 << 16, root_capacity=1 << 12)
+    _, _, _, st = ok.run(1, ev, sc.p_light, ends, rows, etas, t, at, b, t)
+    assert st["roots"] > 4
+    small_roots = A.SubdivisionSolver(box_capacity=1 << 16, root_capacity=4)
+    with pytest.raises(RuntimeError, match="capacity"):
+        small_roots.run(1, ev, sc.p_light, ends, rows, etas, t, at, b, t)
+    small_boxes = A.SubdivisionSolver(box_capacity=rows.shape[0], root_capacity=1 << 12)
+    with pytest.raises(RuntimeError, match="capacity"):
+        small_boxes.run(1, ev, sc.p_light, ends, rows, etas, t, at, b, t)
+    # the solver stays usable after an overflow
+    _, _, _, st2 = ok.run(1, ev, sc.p_light, ends, rows, etas, t, at, b, t)
+    assert st2 == st
