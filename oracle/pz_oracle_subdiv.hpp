@@ -7,9 +7,10 @@
 //   - the domain of a tuple row {q, tri[0..K)} is the unit box of its 2K barycentrics;
 //     split t halves dimension t mod 2K; a box is (depth, path bits);
 //   - a box is dropped when it lies outside a triangle, when the cosines at a vertex rule
-//     the event out (the test of contributableThroughput, pk.h:760-842), or when an
-//     affine bound of the residual of solveConstraints<K> (pk.h:466-592; cross product of
-//     the outgoing direction with the reflected / refracted one) excludes zero;
+//     the event out (the test of contributableThroughput, pk.h:760-842), when an affine
+//     bound of the residual of solveConstraints<K> (pk.h:466-592; cross product of the
+//     outgoing direction with the reflected / refracted one) excludes zero, or when the
+//     joint linear test of two residual components per vertex excludes a root;
 //   - eta^2 - 1 over the bins is one more noise symbol of the bound;
 //   - a box stops splitting at max_depth or when every bounded residual component is
 //     narrower than eps; at such a leaf every bin's value of eta^2 - 1 is substituted
@@ -215,6 +216,59 @@ struct VertexForms {
     float c[3], rad[3], xe[3];
 };
 
+// Joint linear test over the box: rows c0_j + sum_l A_jl e_l + d_j, |d_j| <= r_j,
+// e in [-1, 1]^n.  A solution has e = -Y c0 - Y d + (I - Y A) e for any Y (here A's
+// inverse by Gauss-Jordan with partial pivoting, rounded to nearest); true when that
+// enclosure, rounded outward, misses [-1, 1] in some coordinate.
+template <int n>
+bool linear_excludes(const float (&c0)[n], const float (&A)[n][n], const float (&r)[n])
+{
+    float M[n][2 * n];
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < 2 * n; j++) M[i][j] = j < n ? A[i][j] : (j - n == i ? 1.0f : 0.0f);
+    for (int col = 0; col < n; col++) {
+        int piv = col;
+        float best = std::fabs(M[col][col]);
+        for (int i = col + 1; i < n; i++)
+            if (std::fabs(M[i][col]) > best) {
+                best = std::fabs(M[i][col]);
+                piv = i;
+            }
+        for (int j = 0; j < 2 * n; j++) std::swap(M[col][j], M[piv][j]);
+        if (!(std::fabs(M[col][col]) > 0.0f)) return false;
+        const float inv = 1.0f / M[col][col];
+        for (int j = 0; j < 2 * n; j++) M[col][j] = M[col][j] * inv;
+        for (int i = 0; i < n; i++) {
+            if (i == col) continue;
+            const float f = M[i][col];
+            for (int j = 0; j < 2 * n; j++) M[i][j] = M[i][j] - f * M[col][j];
+        }
+    }
+    for (int i = 0; i < n; i++)
+        for (int j = n; j < 2 * n; j++)
+            if (!std::isfinite(M[i][j])) return false;
+    for (int i = 0; i < n; i++) {
+        float lo = 0.0f, hi = 0.0f, rad = 0.0f;
+        for (int j = 0; j < n; j++) {
+            const float y = M[i][n + j];
+            lo = add_d(lo, mul_d(-y, c0[j]));
+            hi = add_u(hi, mul_u(-y, c0[j]));
+            rad = add_u(rad, mul_u(std::fabs(y), r[j]));
+        }
+        for (int l = 0; l < n; l++) {
+            float sLo = 0.0f, sHi = 0.0f;
+            for (int j = 0; j < n; j++) {
+                sLo = add_d(sLo, mul_d(M[i][n + j], A[j][l]));
+                sHi = add_u(sHi, mul_u(M[i][n + j], A[j][l]));
+            }
+            const float d = i == l ? 1.0f : 0.0f;
+            rad = add_u(rad, std::fmax(sub_u(sHi, d), sub_u(d, sLo)));
+        }
+        if (sub_d(lo, rad) > 1.0f || add_u(hi, rad) < -1.0f) return true;
+    }
+    return false;
+}
+
 // Noise symbols 0 .. 2K-1: the box's parameters; symbol 2K: eta^2 - 1 over the bins.
 template <int K>
 int bound_box(const Triangle* tris, const TriangleAttrib* attribs, F3 pBeg, F3 pEnd, uint32_t events, const Af<2 * K + 1>& em1,
@@ -238,7 +292,8 @@ int bound_box(const Triangle* tris, const TriangleAttrib* attribs, F3 pBeg, F3 p
         X[k + 1] = lin3(v0, e0, e1, u, v);
         Nrm[k] = lin3(n0, ne0, ne1, u, v);
     }
-    bool resolved = true;
+    bool resolved = true, linear = true;
+    float lc0[2 * K], lA[2 * K][2 * K], lr[2 * K];
     for (int k = 0; k < K; k++) {
         if (forms) forms[k].valid = false;
         Af3<N> wi = sub3(X[k], X[k + 1]);
@@ -254,6 +309,7 @@ int bound_box(const Triangle* tris, const TriangleAttrib* attribs, F3 pBeg, F3 p
             std::swap(wi, wo);
         } else if (!(sl >= 0.0f)) {
             resolved = false;
+            linear = false;
             continue;
         }
         const Af<N> NoN = dot3(n, n);
@@ -262,11 +318,11 @@ int bound_box(const Triangle* tris, const TriangleAttrib* attribs, F3 pBeg, F3 p
         if (refract) {
             const Af<N> WoW = dot3(wi, wi);
             const Af<N> kk = add(mul(mul(NoN, WoW), em1), mul(WIoN, WIoN));
-            if (!(lo(kk) >= 0.0f)) { resolved = false; continue; }
+            if (!(lo(kk) >= 0.0f)) { resolved = false; linear = false; continue; }
             const Af<N> g = sub(WIoN, sqrt_af(kk));
             w = add3(Af3<N>{neg(mul(wi.x, NoN)), neg(mul(wi.y, NoN)), neg(mul(wi.z, NoN))}, mul3(n, g));
         } else {
-            if (!(lo(NoN) > 0.0f)) { resolved = false; continue; }
+            if (!(lo(NoN) > 0.0f)) { resolved = false; linear = false; continue; }
             const Af<N> d2 = scale(WIoN, 2.0f);
             w = sub3(mul3(n, d2), mul3(wi, NoN));
         }
@@ -285,7 +341,21 @@ int bound_box(const Triangle* tris, const TriangleAttrib* attribs, F3 pBeg, F3 p
             }
         }
         if (forms) forms[k].valid = true;
+        // the two components of c off wo's largest axis, for the joint test
+        const float ax = std::fabs(wo.x.c), ay = std::fabs(wo.y.c), az = std::fabs(wo.z.c);
+        const int drop = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
+        const Af<N>& ra = drop == 0 ? c.y : c.x;
+        const Af<N>& rb = drop == 2 ? c.y : c.z;
+        lc0[2 * k] = ra.c;
+        lc0[2 * k + 1] = rb.c;
+        for (int i = 0; i < N - 1; i++) {
+            lA[2 * k][i] = ra.x[i];
+            lA[2 * k + 1][i] = rb.x[i];
+        }
+        lr[2 * k] = add_u(ra.r, std::fabs(ra.x[N - 1]));
+        lr[2 * k + 1] = add_u(rb.r, std::fabs(rb.x[N - 1]));
     }
+    if (linear && linear_excludes<2 * K>(lc0, lA, lr)) return kCull;
     return resolved ? kLeaf : kSplit;
 }
 

@@ -12,7 +12,11 @@
 //     taken on the side of the shading normal the solver takes) excludes zero in some
 //     component: no root lies in the box, or
 //   - the sign pattern of the two cosines at some vertex rules out the event over the
-//     whole box, which contributableThroughput (pk.h:760-842) would reject.
+//     whole box, which contributableThroughput (pk.h:760-842) would reject, or
+//   - the joint linear test finds no root: with two residual components per vertex (the
+//     ones off the outgoing direction's largest axis) the affine forms are a 2K x 2K
+//     linear system in the box parameters plus bounded remainders, and a Krawczyk-style
+//     enclosure of its solutions misses the box.
 // A box stops splitting at the depth limit, or when every bounded residual component is
 // narrower than eps (the bound no longer tightens usefully).  Its centre then starts the
 // reference's Newton solve, once per wavelength bin that may hold a root there.  A root
@@ -253,6 +257,84 @@ struct VertexForms {
     float c[3], rad[3], xe[3];
 };
 
+// Joint linear test over the box.  Rows j = 0 .. n-1 model the residual as
+// c0_j + sum_l A_jl e_l + d_j with |d_j| <= r_j and the box parameters e in [-1, 1]^n.  For
+// any matrix Y, a solution satisfies e = -Y c0 - Y d + (I - Y A) e, so e_i lies within
+// -(Y c0)_i -+ (sum_j |Y_ij| r_j + sum_l |(I - Y A)_il|).  When that interval misses
+// [-1, 1] for some i there is no root in the box.  Y is A's inverse by Gauss-Jordan
+// elimination rounded to nearest (any Y keeps the test sound; a singular or non-finite
+// one skips it); every term of the enclosure is rounded outward.
+template <int n>
+PZ_D bool linear_excludes(const float (&c0)[n], const float (&A)[n][n], const float (&r)[n])
+{
+    float M[n][2 * n];
+#pragma unroll
+    for (int i = 0; i < n; i++)
+#pragma unroll
+        for (int j = 0; j < 2 * n; j++) M[i][j] = j < n ? A[i][j] : (j - n == i ? 1.0f : 0.0f);
+#pragma unroll
+    for (int col = 0; col < n; col++) {
+        int piv = col;
+        float best = fabsf(M[col][col]);
+#pragma unroll
+        for (int i = col + 1; i < n; i++)
+            if (fabsf(M[i][col]) > best) {
+                best = fabsf(M[i][col]);
+                piv = i;
+            }
+#pragma unroll
+        for (int i = col + 1; i < n; i++) {  // swap rows col and piv (constant indices: registers)
+            if (i != piv) continue;
+#pragma unroll
+            for (int j = 0; j < 2 * n; j++) {
+                const float t = M[col][j];
+                M[col][j] = M[i][j];
+                M[i][j] = t;
+            }
+        }
+        if (!(fabsf(M[col][col]) > 0.0f)) return false;
+        const float inv = __fdiv_rn(1.0f, M[col][col]);
+#pragma unroll
+        for (int j = 0; j < 2 * n; j++) M[col][j] = __fmul_rn(M[col][j], inv);
+#pragma unroll
+        for (int i = 0; i < n; i++) {
+            if (i == col) continue;
+            const float f = M[i][col];
+#pragma unroll
+            for (int j = 0; j < 2 * n; j++) M[i][j] = __fsub_rn(M[i][j], __fmul_rn(f, M[col][j]));
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < n; i++)
+#pragma unroll
+        for (int j = n; j < 2 * n; j++)
+            if (!isfinite(M[i][j])) return false;
+#pragma unroll
+    for (int i = 0; i < n; i++) {
+        float lo = 0.0f, hi = 0.0f, rad = 0.0f;
+#pragma unroll
+        for (int j = 0; j < n; j++) {
+            const float y = M[i][n + j];
+            lo = __fadd_rd(lo, __fmul_rd(-y, c0[j]));
+            hi = __fadd_ru(hi, __fmul_ru(-y, c0[j]));
+            rad = __fadd_ru(rad, __fmul_ru(fabsf(y), r[j]));
+        }
+#pragma unroll
+        for (int l = 0; l < n; l++) {
+            float sLo = 0.0f, sHi = 0.0f;
+#pragma unroll
+            for (int j = 0; j < n; j++) {
+                sLo = __fadd_rd(sLo, __fmul_rd(M[i][n + j], A[j][l]));
+                sHi = __fadd_ru(sHi, __fmul_ru(M[i][n + j], A[j][l]));
+            }
+            const float d = i == l ? 1.0f : 0.0f;
+            rad = __fadd_ru(rad, fmaxf(__fsub_ru(sHi, d), __fsub_ru(d, sLo)));
+        }
+        if (__fsub_rd(lo, rad) > 1.0f || __fadd_ru(hi, rad) < -1.0f) return true;
+    }
+    return false;
+}
+
 // The bound of one box.  Noise symbols 0 .. 2K-1 are the box's parameters, symbol 2K is
 // eta^2 - 1 over the bins (em1).  forms (may be null) receives each vertex's residual.
 template <int K>
@@ -275,7 +357,8 @@ PZ_D int bound_box(const Chain<K>& ch, float3 pBeg, float3 pEnd, uint32_t events
         X[k + 1] = af3_lin(ch.v0[k], ch.e0[k], ch.e1[k], u, v);
         Nrm[k] = af3_lin(ch.n0[k], ch.ne0[k], ch.ne1[k], u, v);
     }
-    bool resolved = true;
+    bool resolved = true, linear = true;
+    float lc0[2 * K], lA[2 * K][2 * K], lr[2 * K];  // two residual rows per vertex for the joint test
 #pragma unroll
     for (int k = 0; k < K; k++) {
         if (forms) forms[k].valid = false;
@@ -296,6 +379,7 @@ PZ_D int bound_box(const Chain<K>& ch, float3 pBeg, float3 pEnd, uint32_t events
             wo = tmp;
         } else if (!(sl >= 0.0f)) {
             resolved = false;  // the side changes inside the box: no bound at this vertex
+            linear = false;
             continue;
         }
         const Af<N> NoN = af3_dot(n, n);
@@ -307,6 +391,7 @@ PZ_D int bound_box(const Chain<K>& ch, float3 pBeg, float3 pEnd, uint32_t events
             const Af<N> kk = af_add(af_mul(af_mul(NoN, WoW), em1), af_mul(WIoN, WIoN));
             if (!(af_lo(kk) >= 0.0f)) {  // total internal reflection in part of the box
                 resolved = false;
+                linear = false;
                 continue;
             }
             const Af<N> g = af_sub(WIoN, af_sqrt(kk));
@@ -316,6 +401,7 @@ PZ_D int bound_box(const Chain<K>& ch, float3 pBeg, float3 pEnd, uint32_t events
             // (n.n) times the reflection n (wi.n) 2 / (n.n) - wi: the same zeros for n != 0
             if (!(af_lo(NoN) > 0.0f)) {
                 resolved = false;
+                linear = false;
                 continue;
             }
             const Af<N> d2 = af_scale(WIoN, 2.0f);
@@ -338,7 +424,23 @@ PZ_D int bound_box(const Chain<K>& ch, float3 pBeg, float3 pEnd, uint32_t events
             }
         }
         if (forms) forms[k].valid = true;
+        // the two components of c = wo x w that do not lie along wo's largest axis (that
+        // one is about zero everywhere), for the joint test; eta^2 - 1 goes into the radius
+        const float ax = fabsf(wo.x.c), ay = fabsf(wo.y.c), az = fabsf(wo.z.c);
+        const int drop = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
+        const Af<N>& ra = drop == 0 ? c.y : c.x;  // the first kept component
+        const Af<N>& rb = drop == 2 ? c.y : c.z;  // the second
+        lc0[2 * k] = ra.c;
+        lc0[2 * k + 1] = rb.c;
+#pragma unroll
+        for (int i = 0; i < N - 1; i++) {
+            lA[2 * k][i] = ra.x[i];
+            lA[2 * k + 1][i] = rb.x[i];
+        }
+        lr[2 * k] = __fadd_ru(ra.r, fabsf(ra.x[N - 1]));
+        lr[2 * k + 1] = __fadd_ru(rb.r, fabsf(rb.x[N - 1]));
     }
+    if (linear && linear_excludes<2 * K>(lc0, lA, lr)) return kCull;
     return resolved ? kLeaf : kSplit;
 }
 
