@@ -14,9 +14,10 @@
 //   - eta^2 - 1 over the bins is one more noise symbol of the bound;
 //   - a box stops splitting at max_depth or when every bounded residual component is
 //     narrower than eps; at such a leaf every bin's value of eta^2 - 1 is substituted
-//     into the residual forms, and for the bins whose residual may vanish the box centre
-//     starts the Newton solve (solve_constraints in pz_oracle.hpp); a root is kept when it
-//     converged, lies in the box (half-open) and its contributable throughput is positive.
+//     into the residual forms and the joint linear test, and for the bins that pass both
+//     the box centre starts the Newton solve (solve_constraints in pz_oracle.hpp); a root
+//     is kept when it converged, lies in the box (half-open) and its contributable
+//     throughput is positive.
 // Affine arithmetic: central and linear coefficients round to nearest, every rounding
 // error and nonlinear remainder is added to the radius rounded upward.
 //
@@ -220,12 +221,19 @@ struct VertexForms {
 // e in [-1, 1]^n.  A solution has e = -Y c0 - Y d + (I - Y A) e for any Y (here A's
 // inverse by Gauss-Jordan with partial pivoting, rounded to nearest); true when that
 // enclosure, rounded outward, misses [-1, 1] in some coordinate.
+template <int n> struct LinearTest {
+    bool ok;
+    float Y[n][n];
+    float e[n];  // sum_l |(I - Y A)_il|, rounded up
+};
+
 template <int n>
-bool linear_excludes(const float (&c0)[n], const float (&A)[n][n], const float (&r)[n])
+void linear_prepare(LinearTest<n>& T, const float (&A)[n][n])
 {
     float M[n][2 * n];
     for (int i = 0; i < n; i++)
         for (int j = 0; j < 2 * n; j++) M[i][j] = j < n ? A[i][j] : (j - n == i ? 1.0f : 0.0f);
+    T.ok = false;
     for (int col = 0; col < n; col++) {
         int piv = col;
         float best = std::fabs(M[col][col]);
@@ -235,7 +243,7 @@ bool linear_excludes(const float (&c0)[n], const float (&A)[n][n], const float (
                 piv = i;
             }
         for (int j = 0; j < 2 * n; j++) std::swap(M[col][j], M[piv][j]);
-        if (!(std::fabs(M[col][col]) > 0.0f)) return false;
+        if (!(std::fabs(M[col][col]) > 0.0f)) return;
         const float inv = 1.0f / M[col][col];
         for (int j = 0; j < 2 * n; j++) M[col][j] = M[col][j] * inv;
         for (int i = 0; i < n; i++) {
@@ -245,34 +253,70 @@ bool linear_excludes(const float (&c0)[n], const float (&A)[n][n], const float (
         }
     }
     for (int i = 0; i < n; i++)
-        for (int j = n; j < 2 * n; j++)
-            if (!std::isfinite(M[i][j])) return false;
-    for (int i = 0; i < n; i++) {
-        float lo = 0.0f, hi = 0.0f, rad = 0.0f;
         for (int j = 0; j < n; j++) {
-            const float y = M[i][n + j];
-            lo = add_d(lo, mul_d(-y, c0[j]));
-            hi = add_u(hi, mul_u(-y, c0[j]));
-            rad = add_u(rad, mul_u(std::fabs(y), r[j]));
+            if (!std::isfinite(M[i][n + j])) return;
+            T.Y[i][j] = M[i][n + j];
         }
+    for (int i = 0; i < n; i++) {
+        float rad = 0.0f;
         for (int l = 0; l < n; l++) {
             float sLo = 0.0f, sHi = 0.0f;
             for (int j = 0; j < n; j++) {
-                sLo = add_d(sLo, mul_d(M[i][n + j], A[j][l]));
-                sHi = add_u(sHi, mul_u(M[i][n + j], A[j][l]));
+                sLo = add_d(sLo, mul_d(T.Y[i][j], A[j][l]));
+                sHi = add_u(sHi, mul_u(T.Y[i][j], A[j][l]));
             }
             const float d = i == l ? 1.0f : 0.0f;
             rad = add_u(rad, std::fmax(sub_u(sHi, d), sub_u(d, sLo)));
+        }
+        T.e[i] = rad;
+    }
+    T.ok = true;
+}
+
+template <int n>
+bool linear_excludes(const LinearTest<n>& T, const float (&c0)[n], const float (&r)[n])
+{
+    if (!T.ok) return false;
+    for (int i = 0; i < n; i++) {
+        float lo = 0.0f, hi = 0.0f, rad = T.e[i];
+        for (int j = 0; j < n; j++) {
+            const float y = T.Y[i][j];
+            lo = add_d(lo, mul_d(-y, c0[j]));
+            hi = add_u(hi, mul_u(-y, c0[j]));
+            rad = add_u(rad, mul_u(std::fabs(y), r[j]));
         }
         if (sub_d(lo, rad) > 1.0f || add_u(hi, rad) < -1.0f) return true;
     }
     return false;
 }
 
+// a leaf's joint-test rows, kept for the per-bin tests
+template <int K> struct LinearRows {
+    bool valid;
+    LinearTest<2 * K> test;
+    float c[2 * K], xe[2 * K], r[2 * K];
+};
+
+// the joint test for one bin: its eta symbol [elo, ehi] substituted into every row
+template <int K>
+bool bin_linear_excludes(const LinearRows<K>& L, float elo, float ehi)
+{
+    if (!L.valid) return false;
+    float c0[2 * K], r[2 * K];
+    for (int j = 0; j < 2 * K; j++) {
+        const float pl = std::fmin(mul_d(L.xe[j], elo), mul_d(L.xe[j], ehi));
+        const float ph = std::fmax(mul_u(L.xe[j], elo), mul_u(L.xe[j], ehi));
+        const float cl = add_d(L.c[j], pl), ch = add_u(L.c[j], ph);
+        c0[j] = (cl + ch) * 0.5f;
+        r[j] = add_u(L.r[j], std::fmax(sub_u(ch, c0[j]), sub_u(c0[j], cl)));
+    }
+    return linear_excludes<2 * K>(L.test, c0, r);
+}
+
 // Noise symbols 0 .. 2K-1: the box's parameters; symbol 2K: eta^2 - 1 over the bins.
 template <int K>
 int bound_box(const Triangle* tris, const TriangleAttrib* attribs, F3 pBeg, F3 pEnd, uint32_t events, const Af<2 * K + 1>& em1,
-              const float* bl, const float* bh, float eps, VertexForms* forms = nullptr)
+              const float* bl, const float* bh, float eps, VertexForms* forms = nullptr, LinearRows<K>* rows = nullptr)
 {
     constexpr int N = 2 * K + 1;
     for (int k = 0; k < K; k++)
@@ -293,7 +337,7 @@ int bound_box(const Triangle* tris, const TriangleAttrib* attribs, F3 pBeg, F3 p
         Nrm[k] = lin3(n0, ne0, ne1, u, v);
     }
     bool resolved = true, linear = true;
-    float lc0[2 * K], lA[2 * K][2 * K], lr[2 * K];
+    float lc0[2 * K], lA[2 * K][2 * K], lr[2 * K], lxe[2 * K], lrn[2 * K];
     for (int k = 0; k < K; k++) {
         if (forms) forms[k].valid = false;
         Af3<N> wi = sub3(X[k], X[k + 1]);
@@ -354,8 +398,25 @@ int bound_box(const Triangle* tris, const TriangleAttrib* attribs, F3 pBeg, F3 p
         }
         lr[2 * k] = add_u(ra.r, std::fabs(ra.x[N - 1]));
         lr[2 * k + 1] = add_u(rb.r, std::fabs(rb.x[N - 1]));
+        lxe[2 * k] = ra.x[N - 1];
+        lxe[2 * k + 1] = rb.x[N - 1];
+        lrn[2 * k] = ra.r;
+        lrn[2 * k + 1] = rb.r;
     }
-    if (linear && linear_excludes<2 * K>(lc0, lA, lr)) return kCull;
+    if (linear) {
+        LinearTest<2 * K> T;
+        linear_prepare<2 * K>(T, lA);
+        if (linear_excludes<2 * K>(T, lc0, lr)) return kCull;
+        if (rows) {
+            rows->test = T;
+            for (int j = 0; j < 2 * K; j++) {
+                rows->c[j] = lc0[j];
+                rows->xe[j] = lxe[j];
+                rows->r[j] = lrn[j];
+            }
+        }
+    }
+    if (rows) rows->valid = linear;
     return resolved ? kLeaf : kSplit;
 }
 
@@ -450,11 +511,12 @@ void solve_row(uint32_t row, const uint32_t* tuples, uint32_t events, F3 pBeg, c
         }
         stats[2]++;
         VertexForms forms[K];
-        bound_box<K>(tris, attribs, pBeg, pEnd[q], events, em1, bl, bh, P.eps, forms);
+        LinearRows<K> lrows;
+        bound_box<K>(tris, attribs, pBeg, pEnd[q], events, em1, bl, bh, P.eps, forms, &lrows);
         for (int b = 0; b < nBins; b++) {
             float elo, ehi;
             bin_symbol(em1, etas[b] * etas[b] - 1.0f, &elo, &ehi);
-            if (!bin_may_hold_root<K>(forms, elo, ehi)) {
+            if (!bin_may_hold_root<K>(forms, elo, ehi) || bin_linear_excludes<K>(lrows, elo, ehi)) {
                 stats[3]++;
                 continue;
             }

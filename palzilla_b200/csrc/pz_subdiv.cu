@@ -27,8 +27,8 @@
 //   - contributableThroughput, visibility included, is positive.
 // The wavelength bins share one subdivision: eta^2 - 1 over the range of the bins' values
 // is one more noise symbol of the bound, so a box that survives for any bin survives.  At
-// a leaf, each bin's value of that symbol is substituted into the residual forms, and a
-// bin whose residual range then excludes zero gets no Newton solve.
+// a leaf, each bin's value of that symbol is substituted into the residual forms and the
+// joint linear test, and a bin for which either then excludes a root gets no Newton solve.
 //
 // Affine forms: x = c + sum_i x_i e_i + r e_err with |e_i|, |e_err| <= 1; the noise
 // symbols e_i are the box's 2K parameters and eta^2 - 1.  Central and linear coefficients are rounded
@@ -264,14 +264,21 @@ struct VertexForms {
 // [-1, 1] for some i there is no root in the box.  Y is A's inverse by Gauss-Jordan
 // elimination rounded to nearest (any Y keeps the test sound; a singular or non-finite
 // one skips it); every term of the enclosure is rounded outward.
+template <int n> struct LinearTest {
+    bool ok;            // false: A singular or Y not finite (no test)
+    float Y[n][n];      // approximate inverse of A
+    float e[n];         // sum_l |(I - Y A)_il|, rounded up
+};
+
 template <int n>
-PZ_D bool linear_excludes(const float (&c0)[n], const float (&A)[n][n], const float (&r)[n])
+PZ_D void linear_prepare(LinearTest<n>& T, const float (&A)[n][n])
 {
     float M[n][2 * n];
 #pragma unroll
     for (int i = 0; i < n; i++)
 #pragma unroll
         for (int j = 0; j < 2 * n; j++) M[i][j] = j < n ? A[i][j] : (j - n == i ? 1.0f : 0.0f);
+    T.ok = false;
 #pragma unroll
     for (int col = 0; col < n; col++) {
         int piv = col;
@@ -292,7 +299,7 @@ PZ_D bool linear_excludes(const float (&c0)[n], const float (&A)[n][n], const fl
                 M[i][j] = t;
             }
         }
-        if (!(fabsf(M[col][col]) > 0.0f)) return false;
+        if (!(fabsf(M[col][col]) > 0.0f)) return;
         const float inv = __fdiv_rn(1.0f, M[col][col]);
 #pragma unroll
         for (int j = 0; j < 2 * n; j++) M[col][j] = __fmul_rn(M[col][j], inv);
@@ -307,39 +314,81 @@ PZ_D bool linear_excludes(const float (&c0)[n], const float (&A)[n][n], const fl
 #pragma unroll
     for (int i = 0; i < n; i++)
 #pragma unroll
-        for (int j = n; j < 2 * n; j++)
-            if (!isfinite(M[i][j])) return false;
+        for (int j = 0; j < n; j++) {
+            if (!isfinite(M[i][n + j])) return;
+            T.Y[i][j] = M[i][n + j];
+        }
 #pragma unroll
     for (int i = 0; i < n; i++) {
-        float lo = 0.0f, hi = 0.0f, rad = 0.0f;
-#pragma unroll
-        for (int j = 0; j < n; j++) {
-            const float y = M[i][n + j];
-            lo = __fadd_rd(lo, __fmul_rd(-y, c0[j]));
-            hi = __fadd_ru(hi, __fmul_ru(-y, c0[j]));
-            rad = __fadd_ru(rad, __fmul_ru(fabsf(y), r[j]));
-        }
+        float rad = 0.0f;
 #pragma unroll
         for (int l = 0; l < n; l++) {
             float sLo = 0.0f, sHi = 0.0f;
 #pragma unroll
             for (int j = 0; j < n; j++) {
-                sLo = __fadd_rd(sLo, __fmul_rd(M[i][n + j], A[j][l]));
-                sHi = __fadd_ru(sHi, __fmul_ru(M[i][n + j], A[j][l]));
+                sLo = __fadd_rd(sLo, __fmul_rd(T.Y[i][j], A[j][l]));
+                sHi = __fadd_ru(sHi, __fmul_ru(T.Y[i][j], A[j][l]));
             }
             const float d = i == l ? 1.0f : 0.0f;
             rad = __fadd_ru(rad, fmaxf(__fsub_ru(sHi, d), __fsub_ru(d, sLo)));
+        }
+        T.e[i] = rad;
+    }
+    T.ok = true;
+}
+
+// True when no root lies in the box, for rows with centres c0 and radii r.
+template <int n>
+PZ_D bool linear_excludes(const LinearTest<n>& T, const float (&c0)[n], const float (&r)[n])
+{
+    if (!T.ok) return false;
+#pragma unroll
+    for (int i = 0; i < n; i++) {
+        float lo = 0.0f, hi = 0.0f, rad = T.e[i];
+#pragma unroll
+        for (int j = 0; j < n; j++) {
+            const float y = T.Y[i][j];
+            lo = __fadd_rd(lo, __fmul_rd(-y, c0[j]));
+            hi = __fadd_ru(hi, __fmul_ru(-y, c0[j]));
+            rad = __fadd_ru(rad, __fmul_ru(fabsf(y), r[j]));
         }
         if (__fsub_rd(lo, rad) > 1.0f || __fadd_ru(hi, rad) < -1.0f) return true;
     }
     return false;
 }
 
+// The joint test's rows of a leaf, kept for the per-bin tests: the prepared inverse, and
+// per row the centre, the eta^2 - 1 coefficient and the nonlinear radius.
+template <int K> struct LinearRows {
+    bool valid;
+    LinearTest<2 * K> test;
+    float c[2 * K], xe[2 * K], r[2 * K];
+};
+
+// The joint test for one bin: the bin's eta symbol [elo, ehi] substituted into every row
+// (its spread goes into the radius).
+template <int K>
+PZ_D bool bin_linear_excludes(const LinearRows<K>& L, float elo, float ehi)
+{
+    if (!L.valid) return false;
+    float c0[2 * K], r[2 * K];
+#pragma unroll
+    for (int j = 0; j < 2 * K; j++) {
+        const float pl = fminf(__fmul_rd(L.xe[j], elo), __fmul_rd(L.xe[j], ehi));
+        const float ph = fmaxf(__fmul_ru(L.xe[j], elo), __fmul_ru(L.xe[j], ehi));
+        const float cl = __fadd_rd(L.c[j], pl), ch = __fadd_ru(L.c[j], ph);
+        c0[j] = __fmul_rn(__fadd_rn(cl, ch), 0.5f);
+        r[j] = __fadd_ru(L.r[j], fmaxf(__fsub_ru(ch, c0[j]), __fsub_ru(c0[j], cl)));
+    }
+    return linear_excludes<2 * K>(L.test, c0, r);
+}
+
 // The bound of one box.  Noise symbols 0 .. 2K-1 are the box's parameters, symbol 2K is
 // eta^2 - 1 over the bins (em1).  forms (may be null) receives each vertex's residual.
 template <int K>
 PZ_D int bound_box(const Chain<K>& ch, float3 pBeg, float3 pEnd, uint32_t events, const Af<2 * K + 1>& em1,
-                   const float* lo, const float* hi, float eps, VertexForms* forms = nullptr)
+                   const float* lo, const float* hi, float eps, VertexForms* forms = nullptr,
+                   LinearRows<K>* rows = nullptr)
 {
     constexpr int N = 2 * K + 1;
 #pragma unroll
@@ -359,6 +408,7 @@ PZ_D int bound_box(const Chain<K>& ch, float3 pBeg, float3 pEnd, uint32_t events
     }
     bool resolved = true, linear = true;
     float lc0[2 * K], lA[2 * K][2 * K], lr[2 * K];  // two residual rows per vertex for the joint test
+    float lxe[2 * K], lrn[2 * K];                     // their eta coefficients and nonlinear radii
 #pragma unroll
     for (int k = 0; k < K; k++) {
         if (forms) forms[k].valid = false;
@@ -439,8 +489,26 @@ PZ_D int bound_box(const Chain<K>& ch, float3 pBeg, float3 pEnd, uint32_t events
         }
         lr[2 * k] = __fadd_ru(ra.r, fabsf(ra.x[N - 1]));
         lr[2 * k + 1] = __fadd_ru(rb.r, fabsf(rb.x[N - 1]));
+        lxe[2 * k] = ra.x[N - 1];
+        lxe[2 * k + 1] = rb.x[N - 1];
+        lrn[2 * k] = ra.r;
+        lrn[2 * k + 1] = rb.r;
     }
-    if (linear && linear_excludes<2 * K>(lc0, lA, lr)) return kCull;
+    if (linear) {
+        LinearTest<2 * K> T;
+        linear_prepare<2 * K>(T, lA);
+        if (linear_excludes<2 * K>(T, lc0, lr)) return kCull;
+        if (rows) {
+            rows->test = T;
+#pragma unroll
+            for (int j = 0; j < 2 * K; j++) {
+                rows->c[j] = lc0[j];
+                rows->xe[j] = lxe[j];
+                rows->r[j] = lrn[j];
+            }
+        }
+    }
+    if (rows) rows->valid = linear;
     return resolved ? kLeaf : kSplit;
 }
 
@@ -696,13 +764,15 @@ __global__ void __launch_bounds__(kBlock) k_sub_leaf_test(SubArgs a)
         float lo[N], hi[N];
         box_bounds<N>(path, depth, lo, hi);
         VertexForms forms[K];
-        const bool live = bound_box<K>(ch, a.pBeg, a.pEnd[q], a.events, em1, lo, hi, a.eps, forms) != kCull;
+        LinearRows<K> rows;
+        const bool live = bound_box<K>(ch, a.pBeg, a.pEnd[q], a.events, em1, lo, hi, a.eps, forms, &rows) != kCull;
         if (a.nBins <= 64) {
             // the passing bins as a mask, then one warp-wide append for all of them
             uint64_t mask = 0;
             for (uint32_t b = 0; b < a.nBins; b++) {
                 const float2 sym = binSymbol[b];
-                if (live && bin_may_hold_root<K>(forms, sym.x, sym.y)) mask |= 1ull << b;
+                if (live && bin_may_hold_root<K>(forms, sym.x, sym.y) && !bin_linear_excludes<K>(rows, sym.x, sym.y))
+                    mask |= 1ull << b;
             }
             const uint32_t cnt = (uint32_t)__popcll(mask);
             excluded += a.nBins - cnt;
@@ -714,7 +784,8 @@ __global__ void __launch_bounds__(kBlock) k_sub_leaf_test(SubArgs a)
         } else {
             for (uint32_t b = 0; b < a.nBins; b++) {
                 const float2 sym = binSymbol[b];
-                const bool pass = live && bin_may_hold_root<K>(forms, sym.x, sym.y);
+                const bool pass = live && bin_may_hold_root<K>(forms, sym.x, sym.y) &&
+                                  !bin_linear_excludes<K>(rows, sym.x, sym.y);
                 excluded += !pass;
                 const unsigned long long s = warp_append(a.nItems, pass);
                 if (pass) {
