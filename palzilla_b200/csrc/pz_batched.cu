@@ -360,6 +360,15 @@ __global__ void __launch_bounds__(256) k_probe(BatchArgs a)
 }
 
 // ---------------------------------------------------------------- phase 1
+// Adds a per-thread count to a diagnostic counter: a warp sum, then one atomic per warp.
+// Called by all 32 lanes after the kernels' loops.
+PZ_D void flush_count(unsigned long long* counter, unsigned long long v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(counter, v);
+}
+
 template <int K, bool kMulti>
 __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
 {
@@ -368,6 +377,8 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
     const int bc = B / 2;
     auto* recs = reinterpret_cast<PairRec<K>*>(a.records);
     unsigned long long nItems = 0;
+    // diagnostic counts, kept per thread and added once at the end
+    unsigned long long cMode0 = 0, cMode1 = 0, cMode2 = 0, cProbe = 0, cShift = 0, cNoConv = 0;
     for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < nPaths;
          idx += (uint64_t)gridDim.x * blockDim.x) {
         const SceneRef R = item_scene<kMulti>(a, idx);
@@ -498,15 +509,17 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
                     r.mode = 2;
                     r.mask = 0;
                     r.warm = 0;
-                    if (a.counters) atomicAdd(a.counters + kCntFallbackProbe, 1ull);
+                    cProbe++;
                 }
             }
         }
         nItems += (unsigned long long)B;
-        if (a.counters) {
-            atomicAdd(a.counters + r.mode, 1ull);
-            if (r.mode == 2 && !probeFallback)
-                atomicAdd(a.counters + (conv && conv2 ? kCntFallbackShift : kCntFallbackNoConv), 1ull);
+        cMode0 += r.mode == 0;
+        cMode1 += r.mode == 1;
+        cMode2 += r.mode == 2;
+        if (r.mode == 2 && !probeFallback) {
+            cShift += conv && conv2;
+            cNoConv += !(conv && conv2);
         }
         // warp-aggregated append of the items that have work
         const bool keep = r.mode != 0;
@@ -523,10 +536,14 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
             else raise_error(a.status, kErrCapacity);
         }
     }
-    if (a.s.stats) {
-        const uint32_t active = __activemask();
-        for (int o = 16; o > 0; o >>= 1) nItems += __shfl_xor_sync(active, nItems, o);
-        if ((threadIdx.x & 31) == 0) atomicAdd(a.s.stats + 0, nItems);
+    if (a.s.stats) flush_count(a.s.stats + 0, nItems);
+    if (a.counters) {
+        flush_count(a.counters + kCntMode0, cMode0);
+        flush_count(a.counters + kCntMode1, cMode1);
+        flush_count(a.counters + kCntMode2, cMode2);
+        flush_count(a.counters + kCntFallbackProbe, cProbe);
+        flush_count(a.counters + kCntFallbackShift, cShift);
+        flush_count(a.counters + kCntFallbackNoConv, cNoConv);
     }
 }
 
@@ -541,6 +558,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
     const auto* recs = reinterpret_cast<const PairRec<K>*>(a.records);
     const int chunk = a.chunk > 0 ? a.chunk : 1;
     unsigned long long nConv = 0, nContrib = 0;
+    // diagnostic counts, kept per thread and added once at the end
+    unsigned long long cNewton = 0, cPolish = 0, cQueries = 0, cOverflow = 0, cCand = 0;
     unsigned long long j = 0, jEnd = 0;
     for (;;) {
         // the warp takes `chunk` records at a time from the work counter
@@ -596,11 +615,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
                 // solver from the photon's start, so its accept / reject decision is the plain one
                 const bool conv = newton_nl<K>(xs, ch, S.p_light, fd.p, eta, S.events, S.maxIterations,
                                                S.costTolerance, S.earlyTermWarmUp, true, warm ? 1 : 0, &det);
-                if (a.counters) atomicAdd(a.counters + kCntNewton2, 1ull);
+                cNewton++;
                 if (conv) {
                     nConv++;
                     const bool polish = r.polish || (double)det < a.polishDet;
-                    if (polish && a.counters) atomicAdd(a.counters + kCntPolish, 1ull);
+                    cPolish += polish;
                     float3 vtx[K + 2], nrm[K + 2];
                     if (polish)
                         thr = polish_fp64<K>(xs, ch, S.p_light, fd.p, S.events, eta, vtx, nrm);
@@ -636,10 +655,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
                 rad += 1.0e-5f * (1.0f + mag);  // covers the rounding of the slab and box arithmetic
                 const int nc = fat_query(S.nodes, S.tris, root, ra, rb, rad, cand[warp]);
                 __syncwarp();
-                if (lane == 0 && a.counters) {
-                    atomicAdd(a.counters + kCntQueries, 1ull);
-                    if (nc < 0) atomicAdd(a.counters + kCntFatOverflow, 1ull);
-                    else atomicAdd(a.counters + kCntCandidates, (unsigned long long)nc);
+                if (lane == 0) {
+                    cQueries++;
+                    if (nc < 0) cOverflow++;
+                    else cCand += (unsigned long long)nc;
                 }
                 if (thr > 0.0f) {
                     const float3 d = ex::sub3(sb, sa);
@@ -672,14 +691,15 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
         }
     }
     if (a.s.stats) {
-        for (int o = 16; o > 0; o >>= 1) {
-            nConv += __shfl_xor_sync(0xFFFFFFFFu, nConv, o);
-            nContrib += __shfl_xor_sync(0xFFFFFFFFu, nContrib, o);
-        }
-        if (lane == 0) {
-            atomicAdd(a.s.stats + 1, nConv);
-            atomicAdd(a.s.stats + 2, nContrib);
-        }
+        flush_count(a.s.stats + 1, nConv);
+        flush_count(a.s.stats + 2, nContrib);
+    }
+    if (a.counters) {
+        flush_count(a.counters + kCntNewton2, cNewton);
+        flush_count(a.counters + kCntPolish, cPolish);
+        flush_count(a.counters + kCntQueries, cQueries);
+        flush_count(a.counters + kCntFatOverflow, cOverflow);
+        flush_count(a.counters + kCntCandidates, cCand);
     }
 }
 
