@@ -230,10 +230,12 @@ class Frame:
         self.counter = torch.zeros(1, dtype=torch.int32, device=device)
         self.status = torch.zeros(1, dtype=torch.int32, device=device)
         self.stats = torch.zeros(3, dtype=torch.int64, device=device)
+        self.iteration = 0  # the iteration of the last eye pass (its light point)
 
 
 def solve_primary(ds: DeviceScene, frame: Frame, iteration: int = 0, lens=(0.6, 0.05, 0.0), stream=None):
     sc = ds.scene
+    frame.iteration = iteration
     g = ray_generator(sc)
     l = _lib.LensParams(*[float(x) for x in lens])
     _lib.call("pz_solve_primary", _vp(frame.accum), _vp(frame.fd), C.c_int(sc.width), C.c_int(sc.height), C.byref(g),
@@ -265,11 +267,13 @@ def sort_and_reorder(frame: Frame, n_paths: int, sorter: OnesweepSort, stream=No
 
 def solve_desc(ds: DeviceScene, frame: Frame, cache: PathCache, events_str: str, n_paths: int, spectral=None,
                etas=None, stats=None, max_iterations=32, cost_tolerance=1e-10, early_term_warmup=1, exact=False,
-               polish_det=0.0, continuation=False, fold_det=0.0, iteration=0):
-    """Solve descriptor of one event string; the light is the point of this iteration
-    (Scene.light_point)."""
+               polish_det=0.0, continuation=False, fold_det=0.0, iteration=None):
+    """Solve descriptor of one event string; the light is the point of `iteration`
+    (Scene.light_point), by default the iteration of the frame's last eye pass."""
     from .scenes import event_descriptor
     sc = ds.scene
+    if iteration is None:
+        iteration = frame.iteration
     d = _lib.SolveDesc()
     d.K = len(events_str)
     d.events = event_descriptor(events_str)
