@@ -53,17 +53,32 @@ def _newer(target: str, deps) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def _stamp_flags(extra) -> str:
+    """A file recording the extra flags of the objects in _build/; rewritten (so that every
+    object is rebuilt) when they change."""
+    stamp = os.path.join(OBJ, "extra_flags.txt")
+    text = " ".join(extra)
+    if not os.path.exists(stamp) or open(stamp).read() != text:
+        with open(stamp, "w") as f:
+            f.write(text)
+    return stamp
+
+
 def build(verbose: bool = False, jobs: int | None = None) -> str:
+    """Builds the library.  PZ_EXTRA_NVCC_FLAGS (space-separated) adds flags to every unit,
+    e.g. the sort's shape: -DPZ_SORT_THREADS=256 -DPZ_SORT_ITEMS=16 -DPZ_SORT_RANK_MATCH=0
+    -DPZ_SORT_EARLY_COUNTS=1 -DPZ_SORT_MIN_BLOCKS=4 (the defaults)."""
     os.makedirs(OBJ, exist_ok=True)
+    extra = os.environ.get("PZ_EXTRA_NVCC_FLAGS", "").split()
     headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + \
-        glob.glob(os.path.join(ROOT, "include", "*.h"))
+        glob.glob(os.path.join(ROOT, "include", "*.h")) + [_stamp_flags(extra)]
     objs, procs = [], []
     for unit, (srcname, flags) in UNITS.items():
         src = os.path.join(CSRC, srcname)
         obj = os.path.join(OBJ, unit + ".o")
         objs.append(obj)
         if _newer(obj, [src] + headers + [__file__]):
-            cmd = [NVCC] + ARCH + COMMON + flags + ["-c", src, "-o", obj]
+            cmd = [NVCC] + ARCH + COMMON + flags + extra + ["-c", src, "-o", obj]
             if verbose:
                 print(" ".join(cmd), flush=True)
             procs.append((unit, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
