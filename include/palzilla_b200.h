@@ -386,6 +386,17 @@ PZ_API int pz_adjoint_forward(const pz_solve_desc* desc, pz_stream_t stream);
 PZ_API int pz_adjoint_backward(const pz_solve_desc* desc, const float* dloss_dspectral_dev,
                                const int32_t* corner_vertex_dev, float* grad_heights_dev, float* grad_cauchy_dev,
                                pz_stream_t stream);
+/* The same gradients as pz_adjoint_backward (up to the order of the float atomics), in two
+ * kernels: one keeps the accepted, unclamped (path, bin) pairs and their roots in a list
+ * in scratch_dev (a 256-byte header and 32 bytes per pair, pz_adjoint_scratch_bytes(
+ * capacity)), the other differentiates only those.  Pairs beyond the capacity are dropped
+ * and set PZ_DEVICE_ERR_CAPACITY in the scratch status word (pz_scratch_status).  Does not
+ * synchronise. */
+PZ_API size_t pz_adjoint_scratch_bytes(uint64_t capacity);
+PZ_API int pz_adjoint_backward_compact(const pz_solve_desc* desc, const float* dloss_dspectral_dev,
+                                       const int32_t* corner_vertex_dev, float* grad_heights_dev,
+                                       float* grad_cauchy_dev, void* scratch_dev, size_t scratch_bytes,
+                                       pz_stream_t stream);
 
 /* ---------------------------------------------------------------- resolve
  * pack (main_gpu.cu:499-513): accumulator / count -> sRGB OETF -> RGBA8. */

@@ -102,6 +102,8 @@ SIGNATURES = {
     "pz_subdivide_contribute": (i32, [i32, u32, Float3, f32, f32, vp, vp, u64, vp, vp, i32, vp, vp, vp, vp]),
     "pz_adjoint_forward": (i32, [C.POINTER(SolveDesc), vp]),
     "pz_adjoint_backward": (i32, [C.POINTER(SolveDesc), vp, vp, vp, vp, vp]),
+    "pz_adjoint_scratch_bytes": (sz, [u64]),
+    "pz_adjoint_backward_compact": (i32, [C.POINTER(SolveDesc), vp, vp, vp, vp, vp, sz, vp]),
     "pz_resolve": (i32, [vp, vp, i32, vp]),
     "pz_resolve_spectral": (i32, [vp, vp, vp, i32, i32, f32, f32, Float3, vp]),
 }

@@ -341,19 +341,15 @@ struct AdjArgs {
     float* gradCauchy;        // [2]: dL/dA, dL/dB
 };
 
+// The forward's decisions for one (path, bin), recomputed: Newton from the photon's
+// barycentrics, admissibility and visibility, and the clamp.  True (root in x) when the
+// path contributes unclamped, so that it has a gradient.
 template <int K>
-__global__ void __launch_bounds__(128) k_adjoint(AdjArgs a)
+PZ_D bool adj_accept(const AdjArgs& a, uint64_t pathIdx, uint32_t bin, float (&x)[2 * K])
 {
-    constexpr int NX = 2 * K, NP = 3 * K + 1, N = NX + NP;
-    using S = G<N>;
-    const uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t nb = (uint32_t)a.s.nBins;
-    const uint64_t pathIdx = item / nb;
-    const uint32_t bin = (uint32_t)(item % nb);
-    if (pathIdx >= a.s.nPaths) return;
     const SpecularPath sp = a.s.paths[pathIdx];
-    const float g = a.dLdI[(size_t)sp.pixel * nb + bin];
-    if (g == 0.0f) return;
+    if (a.dLdI[(size_t)sp.pixel * nb + bin] == 0.0f) return false;
     const FirstDiffuse fd = a.s.fds[sp.pixel];
     const int4 ti = a.s.cache.tris[sp.cacheIndex];
     const int idx[4] = {ti.x, ti.y, ti.z, ti.w};
@@ -361,27 +357,42 @@ __global__ void __launch_bounds__(128) k_adjoint(AdjArgs a)
     solver::load_chain<K>(ch, a.s.tris, a.s.attribs, idx);
     const float4 q0 = a.s.cache.params[2 * sp.cacheIndex], q1 = a.s.cache.params[2 * sp.cacheIndex + 1];
     const float pp[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-    float x[NX];
 #pragma unroll
-    for (int i = 0; i < NX; i++) x[i] = pp[i];
+    for (int i = 0; i < 2 * K; i++) x[i] = pp[i];
     const float eta = a.s.etas[bin];
     const V3<float> L = solver::v3f<float>(a.s.p_light), P = solver::v3f<float>(fd.p);
     const uint32_t root = __ldg(a.s.root);
-    // the forward's decisions, recomputed
     if (!solver::solve_constraints<float, K>(x, L, P, ch, eta, a.s.events, a.s.maxIterations, a.s.costTolerance,
                                              a.s.earlyTermWarmUp))
-        return;
+        return false;
     const float thr = solver::contributable_throughput<float, K>(x, L, P, ch, a.s.events, a.s.nodes, a.s.tris, root,
                                                                  eta);
-    if (!(0.0f < thr)) return;
-    {
-        const V3<float> v0 = solver::vertex<float, K>(ch, x, 0);
-        const float dadw = solver::dadw<float, K>(L, v0 - L, P, ch, a.s.events, eta);
-        const V3<float> vl = solver::vertex<float, K>(ch, x, K - 1);
-        const float cosv = fmaxf(solver::vdot(solver::vnormalize(vl - P), solver::v3f<float>(fd.ng)), 0.0f);
-        const float c = thr * a.s.lightIntensity / dadw * cosv;
-        if (!(c < a.s.radianceClamp)) return;  // clamped: no gradient
-    }
+    if (!(0.0f < thr)) return false;
+    const V3<float> v0 = solver::vertex<float, K>(ch, x, 0);
+    const float dadw = solver::dadw<float, K>(L, v0 - L, P, ch, a.s.events, eta);
+    const V3<float> vl = solver::vertex<float, K>(ch, x, K - 1);
+    const float cosv = fmaxf(solver::vdot(solver::vnormalize(vl - P), solver::v3f<float>(fd.ng)), 0.0f);
+    const float c = thr * a.s.lightIntensity / dadw * cosv;
+    return c < a.s.radianceClamp;  // clamped: no gradient
+}
+
+// The gradient of one accepted (path, bin) at its root x: implicit-function derivatives
+// of the root, the contribution's forward-mode derivatives, scaled by dL/dI and added to
+// the heights and the Cauchy coefficients.
+template <int K>
+PZ_D void adj_gradient(const AdjArgs& a, uint64_t pathIdx, uint32_t bin, const float (&x)[2 * K])
+{
+    constexpr int NX = 2 * K, NP = 3 * K + 1, N = NX + NP;
+    using S = G<N>;
+    const uint32_t nb = (uint32_t)a.s.nBins;
+    const SpecularPath sp = a.s.paths[pathIdx];
+    const float g = a.dLdI[(size_t)sp.pixel * nb + bin];
+    const FirstDiffuse fd = a.s.fds[sp.pixel];
+    const int4 ti = a.s.cache.tris[sp.cacheIndex];
+    const int idx[4] = {ti.x, ti.y, ti.z, ti.w};
+    solver::Chain<K> ch;
+    solver::load_chain<K>(ch, a.s.tris, a.s.attribs, idx);
+    const float eta = a.s.etas[bin];
     // tangent layout: [0, 2K) barycentrics, [2K, 5K) corner heights, 5K eta
     GChain<K, S> gc;
 #pragma unroll
@@ -449,6 +460,78 @@ __global__ void __launch_bounds__(128) k_adjoint(AdjArgs a)
     atomicAdd(a.gradCauchy + 1, ge * (eta - a.s.cauchyA) / a.s.cauchyB);
 }
 
+
+template <int K>
+__global__ void __launch_bounds__(128) k_adjoint(AdjArgs a)
+{
+    const uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nb = (uint32_t)a.s.nBins;
+    const uint64_t pathIdx = item / nb;
+    const uint32_t bin = (uint32_t)(item % nb);
+    if (pathIdx >= a.s.nPaths) return;
+    float x[2 * K];
+    if (adj_accept<K>(a, pathIdx, bin, x)) adj_gradient<K>(a, pathIdx, bin, x);
+}
+
+// The compact form: k_adjoint_filter keeps the accepted (path, bin) pairs and their roots
+// in a list (warp-aggregated appends); k_adjoint_grad differentiates only those, in full
+// warps.  The filter runs the light solve code at high occupancy; the gradient's register
+// footprint applies only to paths that contribute.
+struct AdjRecord {
+    uint32_t path, bin;
+    float x[4];
+    uint32_t pad[2];
+};
+static_assert(sizeof(AdjRecord) == 32, "AdjRecord layout");
+
+template <int K>
+__global__ void __launch_bounds__(256) k_adjoint_filter(AdjArgs a, AdjRecord* list, unsigned long long* count,
+                                                        uint64_t capacity, uint32_t* status)
+{
+    const uint32_t nb = (uint32_t)a.s.nBins;
+    const uint64_t items = a.s.nPaths * (uint64_t)nb;
+    for (uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; item < items;
+         item += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t pathIdx = item / nb;
+        const uint32_t bin = (uint32_t)(item % nb);
+        float x[2 * K];
+        const bool keep = adj_accept<K>(a, pathIdx, bin, x);
+        const uint32_t active = __activemask();
+        const uint32_t ballot = __ballot_sync(active, keep);
+        const int leader = __ffs(active) - 1;
+        unsigned long long base = 0;
+        if ((int)(threadIdx.x & 31) == leader && ballot) base = atomicAdd(count, (unsigned long long)__popc(ballot));
+        base = __shfl_sync(active, base, leader);
+        if (keep) {
+            const unsigned long long slot = base + __popc(ballot & ((1u << (threadIdx.x & 31)) - 1u));
+            if (slot < capacity) {
+                AdjRecord r;
+                r.path = (uint32_t)pathIdx;
+                r.bin = bin;
+#pragma unroll
+                for (int i = 0; i < 4; i++) r.x[i] = i < 2 * K ? x[i] : 0.0f;
+                r.pad[0] = r.pad[1] = 0;
+                list[slot] = r;
+            } else {
+                raise_error(status, kErrCapacity);
+            }
+        }
+    }
+}
+
+template <int K>
+__global__ void __launch_bounds__(128) k_adjoint_grad(AdjArgs a, const AdjRecord* list,
+                                                      const unsigned long long* count, uint64_t capacity)
+{
+    const uint64_t n = min((uint64_t)*count, capacity);
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const AdjRecord r = list[i];
+        float x[2 * K];
+#pragma unroll
+        for (int j = 0; j < 2 * K; j++) x[j] = r.x[j];
+        adj_gradient<K>(a, r.path, r.bin, x);
+    }
+}
 }  // namespace adjoint
 }  // namespace pz
 
@@ -480,6 +563,21 @@ static cudaError_t launch_adjoint(const adjoint::AdjArgs& a, cudaStream_t s)
     return cudaGetLastError();
 }
 
+template <int K>
+static cudaError_t launch_adjoint_compact(const adjoint::AdjArgs& a, adjoint::AdjRecord* list,
+                                          unsigned long long* count, uint64_t capacity, uint32_t* status,
+                                          cudaStream_t s)
+{
+    const uint64_t items = a.s.nPaths * (uint64_t)a.s.nBins;
+    if (items == 0) return cudaSuccess;
+    const unsigned grid = (unsigned)std::min<uint64_t>((items + 255) / 256, (uint64_t)kNumSMs * 32);
+    adjoint::k_adjoint_filter<K><<<grid, 256, 0, s>>>(a, list, count, capacity, status);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    adjoint::k_adjoint_grad<K><<<kNumSMs * 16, 128, 0, s>>>(a, list, count, capacity);
+    return cudaGetLastError();
+}
+
 extern "C" int pz_adjoint_backward(const pz_solve_desc* desc, const float* dloss_dspectral_dev,
                                    const int32_t* corner_vertex_dev, float* grad_heights_dev, float* grad_cauchy_dev,
                                    pz_stream_t stream)
@@ -506,6 +604,57 @@ extern "C" int pz_adjoint_backward(const pz_solve_desc* desc, const float* dloss
         default: return fail(PZ_ERR_UNSUPPORTED, "pz_adjoint_backward: K = %d (1 or 2 supported)", desc->K);
     }
     if (e != cudaSuccess) return cuda_fail(e, "pz_adjoint_backward");
+    clear_error();
+    return PZ_OK;
+}
+
+namespace {
+constexpr size_t kAdjHeader = 256;  // status | record count
+}
+
+extern "C" size_t pz_adjoint_scratch_bytes(uint64_t capacity)
+{
+    return kAdjHeader + (size_t)capacity * sizeof(adjoint::AdjRecord);
+}
+
+extern "C" int pz_adjoint_backward_compact(const pz_solve_desc* desc, const float* dloss_dspectral_dev,
+                                           const int32_t* corner_vertex_dev, float* grad_heights_dev,
+                                           float* grad_cauchy_dev, void* scratch_dev, size_t scratch_bytes,
+                                           pz_stream_t stream)
+{
+    if (!desc || desc->n_bins < 1 || !desc->etas)
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_adjoint_backward_compact: binned mode (etas, n_bins >= 1) required");
+    if (!dloss_dspectral_dev || !corner_vertex_dev || !grad_heights_dev || !grad_cauchy_dev || !scratch_dev)
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_adjoint_backward_compact: null buffer");
+    if (desc->cauchy_b == 0.0f)
+        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_adjoint_backward_compact: cauchy_b must be non-zero");
+    if (scratch_bytes < pz_adjoint_scratch_bytes(1) || (reinterpret_cast<uintptr_t>(scratch_dev) & 255))
+        return fail(PZ_ERR_SCRATCH_TOO_SMALL, "pz_adjoint_backward_compact: scratch too small or not 256-byte aligned");
+    adjoint::AdjArgs a;
+    int r = solve_args_from_desc(desc, &a.s, "pz_adjoint_backward_compact");
+    if (r != PZ_OK) return r;
+    a.s.nBins = desc->n_bins;
+    a.s.etas = desc->etas;
+    a.dLdI = dloss_dspectral_dev;
+    a.corner = corner_vertex_dev;
+    a.gradHeights = grad_heights_dev;
+    a.gradCauchy = grad_cauchy_dev;
+    char* base = static_cast<char*>(scratch_dev);
+    auto* status = reinterpret_cast<uint32_t*>(base);
+    auto* count = reinterpret_cast<unsigned long long*>(base + 8);
+    auto* list = reinterpret_cast<adjoint::AdjRecord*>(base + kAdjHeader);
+    const uint64_t capacity = (scratch_bytes - kAdjHeader) / sizeof(adjoint::AdjRecord);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(base, 0, 16, s);
+    if (e == cudaSuccess) {
+        switch (desc->K) {
+            case 1: e = launch_adjoint_compact<1>(a, list, count, capacity, status, s); break;
+            case 2: e = launch_adjoint_compact<2>(a, list, count, capacity, status, s); break;
+            default:
+                return fail(PZ_ERR_UNSUPPORTED, "pz_adjoint_backward_compact: K = %d (1 or 2 supported)", desc->K);
+        }
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "pz_adjoint_backward_compact");
     clear_error();
     return PZ_OK;
 }

@@ -32,6 +32,7 @@ class CausticProblem:
         self.n_paths = A.lookup_flatten(self.frame, self.cache, S.event_descriptor(sc.events))
         A.sort_and_reorder(self.frame, self.n_paths, A.OnesweepSort())
         self.lambdas = torch.from_numpy(sc.bin_lambdas().astype(np.float32)).cuda()
+        self.scratch = None
 
     def set_heights(self, heights):
         tris = self.base_tris.clone().view(-1, 3, 3)
@@ -57,15 +58,25 @@ class CausticProblem:
         _lib.call("pz_adjoint_forward", C.byref(d), C.c_void_p(torch.cuda.current_stream().cuda_stream))
         return spectral
 
-    def backward(self, heights, cauchy, grad_spectral):
+    def backward(self, heights, cauchy, grad_spectral, compact: bool = True):
+        """dL/dheights and dL/d(A, B).  compact: pz_adjoint_backward_compact (filter, then
+        differentiate the accepted paths); else the one-kernel pz_adjoint_backward."""
         self.set_heights(heights)
         spectral = torch.zeros(1, device="cuda")
         etas = self.etas(cauchy)
         d = self.desc(cauchy, spectral, etas)
         gh = torch.zeros_like(heights)
         gc = torch.zeros(2, dtype=torch.float32, device="cuda")
-        _lib.call("pz_adjoint_backward", C.byref(d), A._vp(grad_spectral), A._vp(self.corners), A._vp(gh),
-                  A._vp(gc), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        if compact:
+            nbytes = _lib.lib().pz_adjoint_scratch_bytes(self.n_paths * self.sc.n_bins)
+            if self.scratch is None or self.scratch.numel() < nbytes:
+                self.scratch = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+            _lib.call("pz_adjoint_backward_compact", C.byref(d), A._vp(grad_spectral), A._vp(self.corners),
+                      A._vp(gh), A._vp(gc), A._vp(self.scratch), C.c_size_t(self.scratch.numel()), stream)
+        else:
+            _lib.call("pz_adjoint_backward", C.byref(d), A._vp(grad_spectral), A._vp(self.corners), A._vp(gh),
+                      A._vp(gc), stream)
         return gh, gc
 
 

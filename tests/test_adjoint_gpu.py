@@ -189,3 +189,34 @@ def test_gradient_vs_fp64_reference(setup, orc):
     # a global parameter sums ~5 M path derivatives, some of them near caustic folds where
     # the FP32 derivative of 1 / dAdw loses digits: a few percent
     assert _rel(st["grad_c"][0], dA) < 5e-2 and _rel(st["grad_c"][1], dB) < 5e-2
+
+
+def test_compact_backward_equals_one_kernel(setup):
+    """pz_adjoint_backward_compact (filter the accepted paths into a list, then
+    differentiate only those) gives the one-kernel pz_adjoint_backward's gradients, up to
+    the order of the float atomics; a list too small for the accepted paths sets the
+    capacity bit of the scratch status word."""
+    import ctypes as C
+    from palzilla_b200 import _lib
+    from palzilla_b200 import api as A
+    P, h, cauchy = setup["P"], setup["heights"], setup["cauchy"]
+    g = (2.0 * (setup["I"] - setup["target"])).contiguous()
+    gh1, gc1 = P.backward(h, cauchy, g, compact=True)
+    gh0, gc0 = P.backward(h, cauchy, g, compact=False)
+    torch.cuda.synchronize()
+    a, b = gh1.cpu().numpy().astype(np.float64), gh0.cpu().numpy().astype(np.float64)
+    err = np.abs(a - b).max() / np.abs(b).max()
+    errc = np.abs(gc1.cpu().numpy() - gc0.cpu().numpy()) / np.abs(gc0.cpu().numpy())
+    print(f"\ncompact vs one kernel: heights max err {err:.1e} of the largest, cauchy {errc.max():.1e}")
+    assert np.abs(b).max() > 0 and err < 1e-4 and errc.max() < 1e-4
+    # a list of 1,000 pairs: the gradient misses the rest, and the status word says so
+    P.set_heights(h)
+    d = P.desc(cauchy, torch.zeros(1, device="cuda"), P.etas(cauchy))
+    small = torch.empty(_lib.lib().pz_adjoint_scratch_bytes(1000), dtype=torch.uint8, device="cuda")
+    gh2, gc2 = torch.zeros_like(h), torch.zeros(2, device="cuda")
+    _lib.call("pz_adjoint_backward_compact", C.byref(d), A._vp(g), A._vp(P.corners), A._vp(gh2), A._vp(gc2),
+              A._vp(small), C.c_size_t(small.numel()), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    st = C.c_uint32(0)
+    _lib.call("pz_scratch_status", C.c_void_p(small.data_ptr()), C.byref(st),
+              C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert st.value & 0x2
