@@ -60,8 +60,9 @@ def _oracle_images(orc, sc, frame, cache, n, pixels=None):
     fd = frame.fd.cpu().numpy().view(np.float32).reshape(-1, 10)
     bvh = orc.build_bvh(sc.tris)
     K = len(sc.events)
-    f32, _ = orc.render_pairs(K, pairs, gc, fd, bvh, sc, sc.bin_etas())
-    f64, _ = orc.render_pairs(K, pairs, gc, fd, bvh, sc, sc.bin_etas(), dtype=np.float64)
+    # the light point of the frame's iteration (the sphere's area light moves with it)
+    f32, _ = orc.render_pairs(K, pairs, gc, fd, bvh, sc, sc.bin_etas(), iteration=frame.iteration)
+    f64, _ = orc.render_pairs(K, pairs, gc, fd, bvh, sc, sc.bin_etas(), dtype=np.float64, iteration=frame.iteration)
     return f32, f64
 
 
