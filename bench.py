@@ -48,9 +48,10 @@ WORKLOAD = {
 # kernels of this library launched per frame: k_primary, k_photon, k_lookup, sort k_hist + 4 x k_pass,
 # k_reorder, k_probe, k_phase1, k_phase2, k_resolve_spectral
 LAUNCHES_PER_FRAME = 13
-# DRAM bytes (read + write) per work item of k_probe + k_phase1 + k_phase2, from one ncu capture
-# of the first frame of this workload (profiles/sphere_solver_kernels.md): 6322.5 MB / 19.8 M items
-NCU_SOLVE_TRAFFIC_PER_ITEM = 319.3
+# DRAM bytes (read + write) per work item of k_probe + k_phase1 + k_phase2, from one ncu
+# capture of the first frame of this workload (its light sample is the centre):
+# 6971.2 MB / 19.8 M items
+NCU_SOLVE_TRAFFIC_PER_ITEM = 352.1
 
 
 def peaks():
