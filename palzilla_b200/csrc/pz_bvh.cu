@@ -197,14 +197,16 @@ PZ_D void store_node(Node* dst, const uint32_t c[2], const Box b[2], uint32_t pa
     q[3] = make_float4(b[1].hi.y, b[1].hi.z, __uint_as_float(parent), __uint_as_float(context));
 }
 
-// One thread per leaf climbs while it is the second to arrive at a node.  The first
-// arriver leaves its child index and box in the parent's slot; the exchange on the
-// handshake word is acquire-release, so the second arriver sees them.  A finished
-// node is kept in registers until its own parent is known and then written whole.
+// One thread per leaf climbs while it is the second to arrive at a node.  Each arriver
+// leaves its child index and box in its side's 32-byte slot of the parent's pending record
+// (a whole DRAM sector: no partial writes into the node array); the exchange on the
+// handshake word is acquire-release, so the second arriver sees the first one's slot.  A finished node is kept in
+// registers until its own parent is known and then written whole, once.
 __global__ void __launch_bounds__(kBlock) k_build(Node* __restrict__ nodes, uint32_t* __restrict__ rootOut,
                                                   const Tri* __restrict__ tris, uint32_t n,
                                                   const uint8_t* __restrict__ deltas, uint32_t* flags,
-                                                  const unsigned long long* __restrict__ sorted)
+                                                  const unsigned long long* __restrict__ sorted,
+                                                  float4* __restrict__ pendingRecs)
 {
     const uint32_t i_leaf = blockIdx.x * kBlock + threadIdx.x;
     if (n == 0) {
@@ -232,20 +234,21 @@ __global__ void __launch_bounds__(kBlock) k_build(Node* __restrict__ nodes, uint
         const uint32_t parent = goLeft ? (lower - 1) : upper;
         if (pending) store_node(nodes + node_idx(node), pc, pb, make_node(parent, false), pctx);
         pending = false;
-        Node* P = nodes + parent;
-        P->children[goLeft] = node;
-        P->boxes[goLeft] = box;
+        float4* mine = pendingRecs + 4 * (size_t)parent + 2 * goLeft;  // this side's slot
+        __stcg(mine + 0, make_float4(box.lo.x, box.lo.y, box.lo.z, box.hi.x));
+        __stcg(mine + 1, make_float4(box.hi.y, box.hi.z, __uint_as_float(node), 0.0f));
         cuda::atomic_ref<uint32_t, cuda::thread_scope_device> hs(flags[parent]);
         const uint32_t other = hs.exchange(goLeft ? upper : lower, cuda::memory_order_acq_rel);
         if (other == 0xFFFFFFFFu) { isRoot = false; break; }
         lower = min(lower, other);
         upper = max(upper, other);
-        const float* ob = reinterpret_cast<const float*>(&P->boxes[goLeft ^ 1]);
+        const float4* theirs = pendingRecs + 4 * (size_t)parent + 2 * (goLeft ^ 1);
+        const float4 r0 = __ldcg(theirs + 0), r1 = __ldcg(theirs + 1);
         Box o;
-        o.lo = mk3(__ldcg(ob + 0), __ldcg(ob + 1), __ldcg(ob + 2));
-        o.hi = mk3(__ldcg(ob + 3), __ldcg(ob + 4), __ldcg(ob + 5));
+        o.lo = mk3(r0.x, r0.y, r0.z);
+        o.hi = mk3(r0.w, r1.x, r1.y);
         pc[goLeft] = node;
-        pc[goLeft ^ 1] = __ldcg(&P->children[goLeft ^ 1]);
+        pc[goLeft ^ 1] = __float_as_uint(r1.z);
         pb[goLeft] = box;
         pb[goLeft ^ 1] = o;
         pctx = upper < nInternals ? upper : 0xFFFFFFFFu;
@@ -267,6 +270,7 @@ size_t scratch_bytes(uint32_t n)
     b += 2 * (((size_t)n * 8 + 255) & ~(size_t)255);  // keys + tmp
     b += ((size_t)n + 255) & ~(size_t)255;            // deltas
     b += ((size_t)n * 4 + 255) & ~(size_t)255;        // flags
+    b += ((size_t)n * 64 + 255) & ~(size_t)255;       // pending records (two 32-byte slots)
     return b;
 }
 
@@ -285,6 +289,8 @@ Layout layout(void* scratch, uint32_t n)
     L.deltas = reinterpret_cast<uint8_t*>(p);
     p += ((size_t)n + 255) & ~(size_t)255;
     L.flags = reinterpret_cast<uint32_t*>(p);
+    p += ((size_t)n * 4 + 255) & ~(size_t)255;
+    L.pending = reinterpret_cast<float4*>(p);
     return L;
 }
 
@@ -295,7 +301,7 @@ cudaError_t build(const Tri* tris, uint32_t n, uint32_t opt, Node* nodes, uint32
     cudaError_t e = cudaMemsetAsync(L.s, 0, sizeof(Scratch), st);
     if (e != cudaSuccess) return e;
     if (n == 0) {
-        k_build<<<1, kBlock, 0, st>>>(nodes, root, tris, 0, nullptr, nullptr, nullptr);
+        k_build<<<1, kBlock, 0, st>>>(nodes, root, tris, 0, nullptr, nullptr, nullptr, nullptr);
         return cudaGetLastError();
     }
     const int grid = (int)min((uint32_t)(kNumSMs * 8), (n + kBlock - 1) / kBlock);
@@ -308,7 +314,7 @@ cudaError_t build(const Tri* tris, uint32_t n, uint32_t opt, Node* nodes, uint32
     if (stopAfter == Stage::kSorted) return cudaSuccess;
     const int g = (int)((n + kBlock - 1) / kBlock);
     k_deltas<<<g, kBlock, 0, st>>>(L.keys, n, L.deltas, L.flags);
-    k_build<<<g, kBlock, 0, st>>>(nodes, root, tris, n, L.deltas, L.flags, L.keys);
+    k_build<<<g, kBlock, 0, st>>>(nodes, root, tris, n, L.deltas, L.flags, L.keys, L.pending);
     return cudaGetLastError();
 }
 

@@ -19,6 +19,7 @@ struct Layout {
     unsigned long long* tmp;
     uint8_t* deltas;
     uint32_t* flags;
+    float4* pending;  // per internal node, one 32-byte slot per side: an arriver's child and box
 };
 
 enum class Stage { kKeys, kSorted, kAll };
