@@ -247,10 +247,12 @@ __global__ void __launch_bounds__(kBlock) k_build(Node* __restrict__ nodes, uint
         Box o;
         o.lo = mk3(r0.x, r0.y, r0.z);
         o.hi = mk3(r0.w, r1.x, r1.y);
-        pc[goLeft] = node;
-        pc[goLeft ^ 1] = __float_as_uint(r1.z);
-        pb[goLeft] = box;
-        pb[goLeft ^ 1] = o;
+        // children and boxes by side, with selects (constant indices keep them in registers)
+        const uint32_t theirChild = __float_as_uint(r1.z);
+        pc[0] = goLeft ? theirChild : node;
+        pc[1] = goLeft ? node : theirChild;
+        pb[0] = goLeft ? o : box;
+        pb[1] = goLeft ? box : o;
         pctx = upper < nInternals ? upper : 0xFFFFFFFFu;
         pending = true;
         node = make_node(parent, false);
