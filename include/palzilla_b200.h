@@ -233,6 +233,10 @@ typedef struct pz_solve_desc {
     float fold_det;                        /* batched solve: items whose roots have a relative determinant
                                               below this (near a fold of the caustic) are solved bin by bin
                                               from the photon barycentrics; 0 = 1e-2, < 0 = never */
+    float graze_cos;                       /* batched solve: roots where a path segment meets a surface at
+                                              |cos| below this (near-grazing) are polished in FP64 and
+                                              their admissibility is tested in FP64; <= 0 = never (the
+                                              default); no reference counterpart */
 } pz_solve_desc;
 /* One thread per work item, one launch per call: the reference's plain structure. */
 PZ_API int pz_solve_specular_plain(const pz_solve_desc* desc, pz_stream_t stream);

@@ -55,7 +55,7 @@ class SolveDesc(C.Structure):
                 ("radiance_clamp", f32), ("cauchy_a", f32), ("cauchy_b", f32), ("accum", vp), ("spectral", vp),
                 ("etas", vp), ("n_bins", i32), ("max_iterations", i32), ("cost_tolerance", f32),
                 ("early_term_warmup", i32), ("stats", vp), ("exact_arithmetic", i32), ("polish_det", f32),
-                ("continuation", i32), ("fold_det", f32)]
+                ("continuation", i32), ("fold_det", f32), ("graze_cos", f32)]
 
 
 def f3(v) -> Float3:

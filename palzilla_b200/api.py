@@ -267,7 +267,7 @@ def sort_and_reorder(frame: Frame, n_paths: int, sorter: OnesweepSort, stream=No
 
 def solve_desc(ds: DeviceScene, frame: Frame, cache: PathCache, events_str: str, n_paths: int, spectral=None,
                etas=None, stats=None, max_iterations=32, cost_tolerance=1e-10, early_term_warmup=1, exact=False,
-               polish_det=0.0, continuation=False, fold_det=0.0, iteration=None):
+               polish_det=0.0, continuation=False, fold_det=0.0, iteration=None, graze_cos=0.0):
     """Solve descriptor of one event string; the light is the point of `iteration`
     (Scene.light_point), by default the iteration of the frame's last eye pass."""
     from .scenes import event_descriptor
@@ -304,6 +304,7 @@ def solve_desc(ds: DeviceScene, frame: Frame, cache: PathCache, events_str: str,
     d.polish_det = polish_det
     d.continuation = 1 if continuation else 0
     d.fold_det = fold_det
+    d.graze_cos = graze_cos
     return d
 
 

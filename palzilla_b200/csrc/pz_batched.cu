@@ -226,6 +226,24 @@ __device__ __noinline__ float polish_fp64(float* xs, const Chain<K>& ch, float3 
     return (float)t;
 }
 
+// Smallest |cos| between a path segment and the shading normal over the chain's vertices
+// at the root x (the path grazes a surface when it is small).
+template <int K>
+__device__ __noinline__ float min_abs_cos(const Chain<K>& ch, const float* x, float3 p_light, float3 p)
+{
+    float m = 1.0f;
+#pragma unroll
+    for (int k = 1; k <= K; k++) {
+        float3 va, na, v, n, vb, nb;
+        chain_vertex<K>(ch, x, p_light, p, k - 1, va, na);
+        chain_vertex<K>(ch, x, p_light, p, k, v, n);
+        chain_vertex<K>(ch, x, p_light, p, k + 1, vb, nb);
+        m = fminf(m, fabsf(dot(normalize(va - v), n)));
+        m = fminf(m, fabsf(dot(normalize(vb - v), n)));
+    }
+    return m;
+}
+
 template <int K>
 __device__ __noinline__ float dadw_out_of_line(const Chain<K>& ch, const float* xs, float3 p_light, float3 p,
                                                uint32_t events, float eta)
@@ -618,7 +636,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
                 cNewton++;
                 if (conv) {
                     nConv++;
-                    const bool polish = r.polish || (double)det < a.polishDet;
+                    const bool polish = r.polish || (double)det < a.polishDet ||
+                                        (a.grazeCos > 0.0f && min_abs_cos<K>(ch, xs, S.p_light, fd.p) < a.grazeCos);
                     cPolish += polish;
                     float3 vtx[K + 2], nrm[K + 2];
                     if (polish)

@@ -18,6 +18,7 @@ struct BatchArgs {
     uint32_t* status;                  // status word (capacity overflow)
     unsigned long long* counters;      // device u64[kNumCounters] diagnostics (see kCnt*), or null
     double polishDet;                  // FP64 polish below this relative det (<= 0: never)
+    float grazeCos = 0.0f;             // FP64 polish and admissibility below this |cos| (<= 0: never)
     int continuation;                  // 1: refine predicted roots instead of solving from the photon start
     float illDet;                      // relative det below which an item takes per-bin solves (near a fold)
     int chunk = 0;                     // records a phase-2 warp takes per queue access (0: 1)

@@ -254,6 +254,7 @@ extern "C" int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32
     static_assert(64 + 8 * batched::kNumCounters <= 256, "counters live in the 256-byte scratch header");
     b.counters = reinterpret_cast<unsigned long long*>(base + 64);
     b.polishDet = desc->polish_det > 0.0f ? (double)desc->polish_det : 0.0;
+    b.grazeCos = desc->graze_cos > 0.0f ? desc->graze_cos : 0.0f;
     b.continuation = desc->continuation;
     b.illDet = desc->fold_det < 0.0f ? 0.0f : (desc->fold_det == 0.0f ? 1.0e-2f : desc->fold_det);
     if (desc->n_paths == 0) { clear_error(); return PZ_OK; }
@@ -368,6 +369,7 @@ static int multi_args(int K, int n_bins, uint32_t n_scenes, uint64_t total, void
     b->recordCapacity = total;
     b->probes = base + L.probes;
     b->polishDet = 0.0;
+    b->grazeCos = 0.0f;
     b->continuation = 0;
     b->illDet = 1.0e-2f;
     b->scenes = reinterpret_cast<const batched::SceneArgs*>(base + L.table);
