@@ -152,6 +152,17 @@ PZ_D void chain_vertex(const Chain<K>& ch, const float* x, float3 p_light, float
     }
 }
 
+// a[i] by selects (no stack frame for a runtime index)
+template <int N>
+PZ_D float3 pick(const float3 (&a)[N], int i)
+{
+    float3 r = a[0];
+#pragma unroll
+    for (int j = 1; j < N; j++)
+        if (i == j) r = a[j];
+    return r;
+}
+
 // The shadow-ray segment of occluded() (pk.h:88-115): start and end points.
 PZ_D void shadow_segment(float3 from, float3 from_n, float3 to, float3 to_n, float3& a, float3& b)
 {
@@ -640,6 +651,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
 #endif
             float xs[2 * K];
             float thr = 0.0f;
+            // the chain's vertices and shading normals as the admissibility test built them:
+            // the endpoints of the shadow segments (contributableThroughput, pk.h:763-827)
+            float3 vtx[K + 2], nrm[K + 2];
             if (b < B) {
                 const float eta = S.etas[b];
                 const bool warm = r.mode == 1 && (a.continuation || ((r.warm >> b) & 1ull));
@@ -660,7 +674,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
                     const bool polish = r.polish || (double)det < a.polishDet ||
                                         (a.grazeCos > 0.0f && min_abs_cos<K>(ch, xs, S.p_light, fd.p) < a.grazeCos);
                     cPolish += polish;
-                    float3 vtx[K + 2], nrm[K + 2];
                     if (polish)
                         thr = polish_fp64<K>(xs, ch, S.p_light, fd.p, S.events, eta, vtx, nrm);
                     else
@@ -674,10 +687,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
                 const int leader = __ffs(valid) - 1;
                 float3 sa = mk3(0.f, 0.f, 0.f), sb = mk3(0.f, 0.f, 0.f);
                 if (thr > 0.0f) {
-                    float3 v0, n0, v1, n1;
-                    chain_vertex<K>(ch, xs, S.p_light, fd.p, s, v0, n0);
-                    chain_vertex<K>(ch, xs, S.p_light, fd.p, s + 1, v1, n1);
-                    shadow_segment(v0, n0, v1, n1, sa, sb);
+                    shadow_segment(pick<K + 2>(vtx, s), pick<K + 2>(nrm, s), pick<K + 2>(vtx, s + 1),
+                                   pick<K + 2>(nrm, s + 1), sa, sb);
                 }
                 const float3 ra = mk3(__shfl_sync(0xFFFFFFFFu, sa.x, leader), __shfl_sync(0xFFFFFFFFu, sa.y, leader),
                                       __shfl_sync(0xFFFFFFFFu, sa.z, leader));
