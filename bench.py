@@ -44,7 +44,9 @@ WORKLOAD = {
     "ior": "cauchy 1.5 + 4200/nm^2", "image": "1024x1024", "bins": 64, "lambda_nm": [380, 780],
     "photons": 20480 * 205, "events": "TT", "path_cache": 1 << 22,
     "l2": "no flush: every frame streams buffers larger than L2 (PathCache 252 MB, spectral image 268 MB)",
+    "fp64_polish": "batched solve: FP64 polish and admissibility of roots whose relative |det J| is below 1e-6",
 }
+POLISH_DET = 1.0e-6
 # kernels of this library launched per frame: k_primary, k_photon, k_lookup, sort k_hist + 4 x k_pass,
 # k_reorder, k_probe, k_phase1, k_phase2, k_resolve_spectral
 LAUNCHES_PER_FRAME = 13
@@ -192,7 +194,8 @@ class Renderer:
         A, sc = self.A, self.sc
         self.spectral.zero_()
         d = A.solve_desc(self.ds, self.frame, self.cache, sc.events, self.n_paths, spectral=self.spectral,
-                         etas=self.etas, stats=self.stats, exact=exact, iteration=self.iteration)
+                         etas=self.etas, stats=self.stats, exact=exact, iteration=self.iteration,
+                         polish_det=0.0 if plain else POLISH_DET)
         if solve_events:
             solve_events[0].record()
         if plain:
