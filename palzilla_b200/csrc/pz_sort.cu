@@ -77,11 +77,14 @@ PZ_D uint32_t block_exclusive_scan(uint32_t x, uint32_t* ws)
     return wpre + inc - x;
 }
 
+static_assert(kRankMode != 2 || kEarlyCounts, "ranking mode 2 needs early counts");
+
 template <class KeyT, bool kHasVal>
 struct PassSmem {
     KeyT keys[kTile];                 // tile in digit order
     uint32_t vals[kHasVal ? kTile : 1];
     uint32_t off[kWarps][kRadix];     // per-warp digit counts, then per-warp positions
+    uint32_t match[kRankMode == 2 ? kWarps : 1][kRadix];  // per-warp lane masks by digit (ranking mode 2)
     uint32_t gbase[kRadix];           // global destination of the digit run minus its tile start
     uint32_t ws[2][kWarps];
     uint32_t tile;
@@ -92,7 +95,7 @@ template <bool kAllValid>
 PZ_D uint32_t digit_peers(uint32_t d, bool valid)
 {
     const uint32_t vmask = kAllValid ? 0xFFFFFFFFu : __ballot_sync(0xFFFFFFFFu, valid);
-    if (kRankMatch) return __match_any_sync(0xFFFFFFFFu, valid ? d : 0x100u) & vmask;
+    if (kRankMode == 1) return __match_any_sync(0xFFFFFFFFu, valid ? d : 0x100u) & vmask;
     uint32_t peers = vmask;
 #pragma unroll
     for (int b = 0; b < 8; b++) {
@@ -186,7 +189,26 @@ PZ_D void pass_tile(PassSmem<KeyT, kHasVal>& S, const KeyT* __restrict__ kin, Ke
     for (int k = 0; k < kItems; k++) {
         const bool valid = kFull || wbase + k * 32 + lane < n;
         const uint32_t dd = digit_of(key[k], bit);
-        if (kEarlyCounts) {
+        if (kEarlyCounts && kRankMode == 2) {
+            // peers: every valid lane sets its bit in the mask of its digit, then reads it;
+            // the digit's first lane clears the mask for the next item
+            uint32_t* m = S.match[kRankMode == 2 ? warp : 0];
+            if (valid) atomicOr(&m[dd], 1u << lane);
+            __syncwarp();
+            const uint32_t peers = valid ? m[dd] : 0u;
+            const uint32_t before = __popc(peers & ltmask);
+            const uint32_t run = valid ? S.off[warp][dd] : 0u;
+            __syncwarp();
+            if (valid) {
+                S.keys[run + before] = key[k];
+                if (kHasVal) S.vals[run + before] = val[k];
+                if (before == 0) {
+                    S.off[warp][dd] = run + __popc(peers);
+                    m[dd] = 0u;
+                }
+            }
+            __syncwarp();
+        } else if (kEarlyCounts) {
             const uint32_t peers = digit_peers<kFull>(dd, valid);
             const uint32_t before = __popc(peers & ltmask);
             const uint32_t run = valid ? S.off[warp][dd] : 0u;
@@ -254,6 +276,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass(const KeyT* __res
     auto& S = *reinterpret_cast<PassSmem<KeyT, kHasVal>*>(smem_raw);
     if (threadIdx.x == 0) S.tile = atomicAdd(&h->tile_counter[pass], 1u);
     for (int i = threadIdx.x; i < kWarps * kRadix; i += kThreads) (&S.off[0][0])[i] = 0;
+    if (kRankMode == 2)
+        for (int i = threadIdx.x; i < kWarps * kRadix; i += kThreads) (&S.match[0][0])[i] = 0;
     __syncthreads();
     const uint32_t tile = S.tile;
     if ((uint64_t)(tile + 1) * kTile <= n)

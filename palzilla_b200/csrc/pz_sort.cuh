@@ -24,30 +24,31 @@ namespace pz {
 namespace sort {
 
 // Compile-time shape of the digit pass: threads per tile, items per thread, ranking by
-// warp ballots (0) or match.any (1), digit counts before ranking (1) or from the ranking
-// (0), minimum blocks per SM.  A sweep of eight shapes on 2^24 64-bit keys (4 digit
-// passes, L2 flushed) found these defaults (0.486 ms) within 2% of the fastest (20 items
-// and 3 blocks: 0.478 ms); match.any ranking took 0.726 ms.  Override them through the
-// build (PZ_EXTRA_NVCC_FLAGS).
+// warp ballots (0), match.any (1) or lane bits OR-ed into per-warp digit masks in shared
+// memory (2, with early counts only), digit counts before ranking (1) or from the
+// ranking (0), minimum blocks per SM.  Sweeps on 2^24 64-bit keys (4 digit passes, L2
+// flushed, median of 7) chose the defaults: masks in shared memory, 20 items, 3 blocks
+// (0.460 ms); the best ballot shape took 0.478 ms, 16 items with 4 blocks 0.482 ms, and
+// match.any 0.726 ms.  Override them through the build (PZ_EXTRA_NVCC_FLAGS).
 #ifndef PZ_SORT_THREADS
 #define PZ_SORT_THREADS 256
 #endif
 #ifndef PZ_SORT_ITEMS
-#define PZ_SORT_ITEMS 16
+#define PZ_SORT_ITEMS 20
 #endif
 #ifndef PZ_SORT_RANK_MATCH
-#define PZ_SORT_RANK_MATCH 0
+#define PZ_SORT_RANK_MATCH 2
 #endif
 #ifndef PZ_SORT_EARLY_COUNTS
 #define PZ_SORT_EARLY_COUNTS 1
 #endif
 #ifndef PZ_SORT_MIN_BLOCKS
-#define PZ_SORT_MIN_BLOCKS 4
+#define PZ_SORT_MIN_BLOCKS 3
 #endif
 constexpr int kThreads = PZ_SORT_THREADS;
 constexpr int kWarps = kThreads / 32;
 constexpr int kItems = PZ_SORT_ITEMS;
-constexpr bool kRankMatch = PZ_SORT_RANK_MATCH != 0;
+constexpr int kRankMode = PZ_SORT_RANK_MATCH;
 constexpr bool kEarlyCounts = PZ_SORT_EARLY_COUNTS != 0;
 constexpr int kMinBlocks = PZ_SORT_MIN_BLOCKS;
 constexpr int kTile = kThreads * kItems;  // items per tile

@@ -12,7 +12,7 @@ from palzilla_b200.api import OnesweepSort
 
 pytestmark = pytest.mark.gpu
 
-SIZES = [1, 2, 31, 255, 4095, 4096, 4097, 3 * 4096 + 1, 65536 + 17, 1 << 20]
+SIZES = [1, 2, 31, 255, 4095, 4096, 4097, 3 * 4096 + 1, 5119, 5120, 5121, 3 * 5120 + 1, 65536 + 17, 1 << 20]
 
 
 def _to_dev(a):
