@@ -269,6 +269,38 @@ def lens_scene(side: int = 64, seed: int = 1, amplitude: float = 0.01, events: s
                  width=width, height=height)
 
 
+def blocker_slab(n: int, seed: int, y0: float, y1: float, extent: float, size=(0.03, 0.08)):
+    """n diffuse triangles with a vertex uniform in [-extent/2, extent/2] x [y0, y1] x
+    [-extent/2, extent/2] and two edges of length U[size] in random directions: opaque
+    occluders for the visibility tests."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    v0 = np.stack([rng.uniform(-extent / 2, extent / 2, n), rng.uniform(y0, y1, n),
+                   rng.uniform(-extent / 2, extent / 2, n)], -1)
+    t = np.empty((n, 3, 3), np.float64)
+    t[:, 0] = v0
+    for k in (1, 2):
+        d = rng.standard_normal((n, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        t[:, k] = v0 + d * rng.uniform(size[0], size[1], (n, 1))
+    ng = np.cross(t[:, 1] - t[:, 0], t[:, 2] - t[:, 0])
+    ng /= np.maximum(np.linalg.norm(ng, axis=1, keepdims=True), 1e-30)
+    return t.reshape(-1, 9).astype(np.float32), _attribs(np.repeat(ng[:, None, :], 3, 1), MATERIAL_DIFFUSE)
+
+
+def occluded_lens_scene(side: int = 40, seed: int = 21, n_blockers: int = 300, events: str = "TT", n_bins: int = 16,
+                        width: int = 128, height: int = 128) -> Scene:
+    """lens_scene with a slab of small opaque triangles between the light and the lens
+    (y in [1.2, 2.0] over the central 0.8 x 0.8), so that part of the light segments of
+    the specular paths are occluded.  The camera below the lens does not see the slab, so
+    the eye pass is the one of the open lens.  The blockers come after the lens and
+    receiver triangles: triangle indices of the open lens keep their meaning."""
+    base = lens_scene(side=side, seed=seed, events=events, n_bins=n_bins, width=width, height=height)
+    bt, ba = blocker_slab(n_blockers, seed + 7, 1.2, 2.0, 0.8)
+    tris, att = _combine([(base.tris, base.attribs), (bt, ba)])
+    return Scene(name=f"occluded{side}", tris=tris, attribs=att, camera=base.camera, events=events, n_bins=n_bins,
+                 width=width, height=height)
+
+
 def stacked_lens_scene(sheets: int = 4, side: int = 24, seed: int = 1, amplitude: float = 0.01, n_bins: int = 8,
                        width: int = 96, height: int = 96) -> Scene:
     """Two heightfield lenses stacked over the receiver, for chains of 3 and 4 refractions:

@@ -7,7 +7,8 @@ own CPU code) up to the order of the float atomics: relative RMSE <= 1e-5.  Agai
 plain FMA build it differs exactly as much as that build differs from the oracle (FP32
 accept / reject flips at triangle edges and caustic folds).  The FP64 error of every image
 is printed and bounded.  Scenes: single-refraction heightfield lens (T), two-sheet lens
-(TT), and 20,000 random pixels of the dispersive sphere frame (icosphere-5, 64 bins).
+(TT), the two-sheet lens under a slab of opaque blockers, and 20,000 random pixels of the
+dispersive sphere frame (icosphere-5, 64 bins).
 """
 import ctypes as C
 
@@ -133,6 +134,38 @@ def test_batched_fp64_grazing(orc):
     # a threshold no path reaches leaves the image as it is
     img_0 = _solve(ds, frame, cache, sc, n, "batched", graze_cos=0.1)
     assert _rel(img_0, base) < 1e-6
+
+
+def test_batched_occluded_lens(orc):
+    """Opaque blockers between the light and a two-sheet lens: the warp's shared shadow
+    queries and each lane's candidate tests must reach the visibility decisions of the
+    plain path (one any-hit walk per path segment) and of the oracle.  The blockers come
+    after the lens and receiver triangles, so the same (pixel, tuple) pairs rendered by the
+    oracle in the open lens show that the blockers take light away."""
+    sc = S.occluded_lens_scene(side=40, seed=21, n_blockers=300, events="TT")
+    ds, frame, cache, n = _prepare(sc)
+    assert n > 1000
+    scratch = A.Scratch()
+    img_b = _solve(ds, frame, cache, sc, n, "batched", scratch)
+    img_x = _solve(ds, frame, cache, sc, n, "exact")
+    f32, f64 = _oracle_images(orc, sc, frame, cache, n)
+    open_sc = S.lens_scene(side=40, seed=21, events="TT", n_bins=sc.n_bins, width=sc.width, height=sc.height)
+    pairs = frame.paths[: n * 8].cpu().numpy().view(np.int32).reshape(-1, 2).copy()
+    fd = frame.fd.cpu().numpy().view(np.float32).reshape(-1, 10)
+    f32_open, _ = orc.render_pairs(2, pairs, cache.to_host(), fd, orc.build_bvh(open_sc.tris), open_sc,
+                                   sc.bin_etas(), iteration=frame.iteration)
+    cnt = A.batched_counters(scratch)
+    kept = float(f32.sum() / f32_open.sum())
+    r = {"batched_vs_plain_exact": _rel(img_b, img_x), "batched_vs_oracle": _rel(img_b, f32),
+         "batched_vs_fp64": _rel(img_b, f64), "oracle_vs_fp64": _rel(f32, f64)}
+    print(f"\n[occluded TT] n={n} light kept by the blockers {kept:.4f} " +
+          " ".join(f"{k}={v:.2e}" for k, v in r.items()) +
+          f" queries={cnt['vis_queries']} candidates={cnt['vis_candidates']} overflow={cnt['vis_overflow']}")
+    assert scratch.status() == 0
+    assert kept < 1.0  # the blockers occlude some of the solved paths
+    assert r["batched_vs_plain_exact"] <= 1e-5
+    assert r["batched_vs_oracle"] <= 1e-5
+    assert r["batched_vs_fp64"] <= max(1.01 * r["oracle_vs_fp64"], 1e-5)
 
 
 def test_batched_sphere_sample(orc):
