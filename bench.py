@@ -189,7 +189,7 @@ class Renderer:
         self.n_paths = A.lookup_flatten(fr, self.cache, self.ev)
         A.sort_and_reorder(fr, self.n_paths, self.sorter)
 
-    def solve(self, plain: bool = False, exact: bool = False, solve_events=None):
+    def solve(self, plain: bool = False, exact: bool = True, solve_events=None):
         """Specular solve of the prepared work list into a cleared spectral image, then resolve."""
         A, sc = self.A, self.sc
         self.spectral.zero_()
@@ -262,12 +262,14 @@ def run_ours(args):
     def rel(a, b):
         return float(torch.sqrt(((a - b).double() ** 2).mean()) / torch.sqrt((b.double() ** 2).mean()))
     imgs = {}
-    for tag, plain, exact in (("plain_exact", True, True), ("plain", True, False), ("batched", False, False)):
+    # "plain" is the product's plain solve (no FMA contraction: the reference's float arithmetic),
+    # the denominator of the speed-up; "plain_fma" is its opt-in FMA-contracted build
+    for tag, plain, exact in (("plain", True, True), ("plain_fma", True, False), ("batched", False, True)):
         R.solve(plain=plain, exact=exact)
         torch.cuda.synchronize()
         imgs[tag] = (R.spectral.clone(), R.rgb[:, :3].clone())
     rmse = {}
-    for a, b in (("batched", "plain_exact"), ("batched", "plain"), ("plain", "plain_exact")):
+    for a, b in (("batched", "plain"), ("plain_fma", "plain")):
         rmse[f"{a}_vs_{b}"] = {"spectral": rel(imgs[a][0], imgs[b][0]), "rgb": rel(imgs[a][1], imgs[b][1])}
     del imgs
 

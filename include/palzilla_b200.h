@@ -90,12 +90,17 @@ PZ_API int pz_onesweep_sort(void* keys_dev, uint32_t* values_dev, void* tmp_keys
 
 /* No reference counterpart (the reference's OnesweepSort owns and allocates its scratch).
  * The same sort as pz_onesweep_sort, with the scratch taken from a static device array of
- * this library (2,113,536 bytes per device: the 16 KiB header and look-back rows for
- * PZ_ONESWEEP_STATIC_MAX_KEYS keys), for callers that cannot allocate device memory at call
- * time.  n > PZ_ONESWEEP_STATIC_MAX_KEYS is rejected with PZ_ERR_SCRATCH_TOO_SMALL before
- * any device work.  The first call on a device looks up the array's address (and may load
- * the module), so make it before any stream capture.  Nothing has to be zeroed by the
- * caller: each call clears what it uses on `stream`.  All calls on one device share the
+ * this library instead of a caller buffer, for callers that cannot allocate device memory
+ * at call time.  The array holds the 16 KiB header and the look-back rows for
+ * PZ_ONESWEEP_STATIC_MAX_KEYS keys at the build's tile size: 1,695,744 bytes with the
+ * default 5,120-key tiles, held in every CUDA context that loads the library until it
+ * exits.  n > PZ_ONESWEEP_STATIC_MAX_KEYS is rejected with PZ_ERR_SCRATCH_TOO_SMALL before
+ * any device work.  Every call looks up the array's address in the CUDA context current on
+ * the calling thread (a __device__ array has one address per context), so hosts that make
+ * their own contexts or re-create one after cudaDeviceReset are served too.  That look-up
+ * allocates nothing, but the first call in a context may load the library's module into
+ * it, so make that first call before any stream capture.  Nothing has to be zeroed by the
+ * caller: each call clears what it uses on `stream`.  All calls in one context share the
  * array: calls whose GPU work can overlap (unordered streams) race; order them on one
  * stream.  When status_dev != NULL the sort's status word (PZ_DEVICE_ERR_* bits, 0 = ok)
  * is copied there on `stream` after the sort. */
@@ -222,7 +227,10 @@ typedef struct pz_solve_desc {
     float cost_tolerance;                  /* 1e-10 */
     int early_term_warmup;                 /* 1 */
     unsigned long long* stats;             /* device u64[3]: items solved, converged, contributing (or NULL) */
-    int exact_arithmetic;                  /* plain solve: 1 = no FMA contraction (bit-compatible with the CPU oracle) */
+    int fma_contraction;                   /* plain solve: 0 (the default) = no FMA contraction, the reference's float
+                                              arithmetic of the CPU code bit for bit; 1 = contracted multiply-adds
+                                              (faster, but edge and fold decisions move: about 4e-3 relative RMSE
+                                              on the dispersive-sphere image) */
     float polish_det;                      /* batched solve: FP64 polish of roots whose relative determinant
                                               prod|R_ii| / max|R_ii|^(2K) is below this; <= 0 = never (the
                                               default: the image then follows the reference's float
@@ -237,6 +245,13 @@ typedef struct pz_solve_desc {
                                               |cos| below this (near-grazing) are polished in FP64 and
                                               their admissibility is tested in FP64; <= 0 = never (the
                                               default); no reference counterpart */
+    float* roots;                          /* optional, NULL = none: the root of every (item, bin) solve that
+                                              converged, 8 floats at [(item * n_bins + bin) * 8] (2K used; n_bins
+                                              is 1 in reference mode).  Entries of bins that were not solved or
+                                              did not converge are left as they were: fill the buffer with NaN
+                                              first to tell them apart.  The batched solve solves only the bins
+                                              that can contribute (a bin whose root lies outside a triangle is
+                                              skipped) */
 } pz_solve_desc;
 /* One thread per work item, one launch per call: the reference's plain structure. */
 PZ_API int pz_solve_specular_plain(const pz_solve_desc* desc, pz_stream_t stream);
@@ -257,6 +272,21 @@ PZ_API size_t pz_solve_batched_scratch_bytes(int K, uint64_t max_paths);
  * shift over the band was too large. */
 PZ_API int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32_t* n_paths_dev, void* scratch_dev,
                                      size_t scratch_bytes, int blocks_per_sm, pz_stream_t stream);
+
+/* Batch of device-side solveConstraints<K> calls (pk.h:466-592) through the device-callable
+ * solver of palzilla_b200_device.cuh, one per item, in the reference's float arithmetic (no
+ * FMA contraction: equal to its CPU code bit for bit).  Item i solves the chain of triangles
+ * tuples_dev[i*K .. i*K+K) (indices into triangles_dev / attribs_dev) from p_beg to
+ * p_end_dev[i] at eta etas_dev[i], starting from the 2K barycentrics params_dev[i*2K ..],
+ * which are overwritten with the solver's last iterate (the root when it converged).
+ * converged_dev[i] (may be NULL) = 1 when the cost tolerance was reached; iters_dev[i] (may
+ * be NULL) = the last iteration passed to the end-of-iteration callback (-1 when the solve
+ * was rejected at a triangle edge before any callback). */
+PZ_API int pz_solve_constraints(int K, uint32_t events, pz_float3 p_beg, const int32_t* tuples_dev,
+                                const pz_float3* p_end_dev, const float* etas_dev, uint32_t n,
+                                const pz_triangle* triangles_dev, const pz_triangle_attrib* attribs_dev,
+                                int max_iterations, float cost_tolerance, int early_term_warmup, float* params_dev,
+                                uint8_t* converged_dev, int32_t* iters_dev, pz_stream_t stream);
 
 /* ---------------------------------------------------------------- batches of scenes
  * No reference counterpart.  Many scenes (each with its own triangles, BVH, PathCache,
@@ -378,7 +408,7 @@ PZ_API int pz_subdivide_contribute(int K, uint32_t events, pz_float3 p_beg, floa
 /* ---------------------------------------------------------------- adjoint
  * No reference counterpart.  A forward / backward pair for gradients of a loss on the
  * binned spectral image.  Forward: the plain binned solve in the reference's arithmetic
- * (exact_arithmetic is implied) into desc->spectral.  Backward (same descriptor and work
+ * (fma_contraction is ignored) into desc->spectral.  Backward (same descriptor and work
  * list, geometry unchanged since the forward): recomputes each path's root from the
  * photon's barycentrics, and for every accepted, unclamped path adds
  * dL/dI[pixel][bin] * dI/dp to the gradients, by the implicit-function theorem at the

@@ -8,8 +8,9 @@
 # class (lines 1171-1704 plus the matching #endif on line 2224), which needs the
 # absent graphics/Alembic libraries.  No reference source is copied into the repo.
 set -euo pipefail
-REF_DIR=${REF_DIR:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
+# the reference sources: $REF_DIR, else a directory named "reference" beside the repository
+REF_DIR=${REF_DIR:-$(cd "$HERE/../.." && pwd)/reference}
 OUT=$HERE/_ref
 if [ ! -f "$REF_DIR/pk.h" ]; then
   echo "build_ref.sh: reference sources not found at $REF_DIR; skipping" >&2

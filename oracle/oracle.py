@@ -48,11 +48,17 @@ def build_oracle(force: bool = False) -> None:
         subprocess.run(["make", "-C", HERE, "-s"], check=True)
 
 
+def ref_dir() -> str:
+    """Where the reference sources are looked for: $REF_DIR, else a directory named
+    "reference" beside this repository's root."""
+    return os.environ.get("REF_DIR", os.path.normpath(os.path.join(HERE, "..", "..", "reference")))
+
+
 def build_ref() -> bool:
     """Compile the reference's CPU code when its sources are present; True if the library exists."""
     script = os.path.join(HERE, "build_ref.sh")
-    if os.path.isdir(os.environ.get("REF_DIR", "/root/reference")):
-        subprocess.run([script], check=True, stdout=subprocess.DEVNULL)
+    if os.path.isdir(ref_dir()):
+        subprocess.run([script], check=True, stdout=subprocess.DEVNULL, env=dict(os.environ, REF_DIR=ref_dir()))
     return os.path.exists(REF_SO)
 
 
@@ -278,6 +284,50 @@ class CpuLib:
                  C.c_int(nb), C.c_int(max_iter), C.c_float(tol), C.c_int(warmup), _p(spectral), _p(stats)]
         self.f("render_pairs", C.c_int)(*args)
         return spectral, stats
+
+    def render_pairs_rgb(self, K, pairs, cache, first_diffuse, bvh, scene, max_iter=32, tol=1e-10, warmup=1,
+                         dtype=np.float32, iteration=0):
+        """The reference's own solve mode (solveSpecularPath<K>, main_gpu.cu:418-483): each
+        (pixel, tuple) pair at its pixel's sampled wavelength, RGB added to a float4
+        accumulator per pixel (w = 0 here).  Returns (accum (npx, 4), stats)."""
+        pairs = np.ascontiguousarray(pairs, np.int32)
+        fd = np.ascontiguousarray(first_diffuse, np.float32)
+        accum = np.zeros((fd.shape[0], 4), np.float32)
+        stats = np.zeros(3, np.int64)
+        from palzilla_b200.scenes import event_descriptor
+        args = [C.c_int(K)]
+        if self.prefix == "pzo":
+            args.append(C.c_int(0 if dtype == np.float32 else 1))
+        args += [_p(pairs), C.c_int64(pairs.shape[0]), _p(cache["tris"]), _p(cache["params"]), _p(fd),
+                 _p(bvh["nodes"]), C.c_uint32(bvh["root"]), _p(scene.tris), _p(scene.attribs),
+                 _p(_light(scene, iteration)), C.c_float(scene.light_intensity), C.c_float(scene.radiance_clamp),
+                 C.c_uint32(event_descriptor(scene.events)), C.c_float(scene.cauchy_a), C.c_float(scene.cauchy_b),
+                 C.c_int(max_iter), C.c_float(tol), C.c_int(warmup), _p(accum), _p(stats)]
+        self.f("render_pairs_rgb", C.c_int)(*args)
+        return accum, stats
+
+    def cmf(self, which: int, nm: np.ndarray) -> np.ndarray:
+        """CIE 2015 10-degree functions (pk.h:960-1012): 0 x, 1 y, 2 z, 3 pdf of the sampled
+        wavelength, 4 its inverse CDF."""
+        fn = self.f("cmf", C.c_float)
+        return np.array([fn(C.c_int(which), C.c_float(float(x))) for x in np.asarray(nm, np.float32)], np.float32)
+
+    def pack(self, accum) -> np.ndarray:
+        """pack (main_gpu.cu:499-513): RGBA8 of accumulator / count."""
+        accum = np.ascontiguousarray(accum, np.float32)
+        out = np.zeros(accum.shape[0], np.uint32)
+        self.f("pack")(_p(accum), C.c_int(accum.shape[0]), _p(out))
+        return out
+
+    def resolve_spectral(self, spectral, lambda_min, lambda_max, albedo):
+        """Binned spectral image -> (linear sRGB (n, 4), RGBA8 (n,))."""
+        spectral = np.ascontiguousarray(spectral, np.float32)
+        n, nb = spectral.shape
+        rgb = np.zeros((n, 4), np.float32)
+        px = np.zeros(n, np.uint32)
+        self.f("resolve_spectral")(_p(spectral), C.c_int(n), C.c_int(nb), C.c_float(lambda_min),
+                                   C.c_float(lambda_max), _p(np.asarray(albedo, np.float32)), _p(rgb), _p(px))
+        return rgb, px
 
     def render_each(self, K, pairs, cache, first_diffuse, bvh, scene, etas, max_iter=32, tol=1e-10, warmup=1,
                     dtype=np.float64, iteration=0):

@@ -452,6 +452,58 @@ static void render_pairs(const int32_t* pairs, int64_t nPairs, const int32_t* sl
     stats[1] = conv;
     stats[2] = contrib;
 }
+// The reference's own solve mode (solveSpecularPath<K>, main_gpu.cu:418-483): one thread per
+// (pixel, tuple) with the pixel's sampled wavelength from the eye pass (FirstDiffuse.lambda),
+// eta = cauchy(lambda), and the clamped contribution weighted into linear sRGB by the CMFs
+// and the wavelength pdf, added to the pixel's float4 accumulator (RGB; w untouched).
+template <class T, int K>
+static void render_pairs_rgb(const int32_t* pairs, int64_t nPairs, const int32_t* slotTris, const float* slotParams,
+                             const float* firstDiffuse, const InternalNode* nodes, uint32_t root, const Triangle* tris,
+                             const TriangleAttrib* attribs, F3 L, float lightIntensity, float radianceClamp,
+                             uint32_t events, float cauchyA, float cauchyB, int maxIter, float tol, int warmup,
+                             float* accum, int64_t* stats)
+{
+    int64_t conv = 0, contrib = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : conv, contrib)
+    for (int64_t q = 0; q < nPairs; q++) {
+        int px = pairs[2 * q], slot = pairs[2 * q + 1];
+        const float* fd = firstDiffuse + 10 * (size_t)px;
+        V3<T> p = mk((T)fd[0], (T)fd[1], (T)fd[2]);
+        V3<T> n = mk((T)fd[3], (T)fd[4], (T)fd[5]);
+        const F3 R = mk(fd[6], fd[7], fd[8]);
+        const float lambda = fd[9];
+        Triangle tk[K];
+        TriangleAttrib ak[K];
+        for (int k = 0; k < K; k++) { tk[k] = tris[slotTris[4 * slot + k]]; ak[k] = attribs[slotTris[4 * slot + k]]; }
+        T prm[2 * K];
+        for (int i = 0; i < 2 * K; i++) prm[i] = (T)slotParams[8 * slot + i];
+        const float p_lambda = cmf_y_pdf(lambda);
+        const T eta = (T)cauchy(cauchyA, cauchyB, lambda);
+        V3<T> Lt = mk((T)L.x, (T)L.y, (T)L.z);
+        if (!solve_constraints<T, K>(prm, Lt, p, tk, ak, eta, events, maxIter, (T)tol, warmup)) continue;
+        conv++;
+        T thr = contributable_throughput<T, K>(prm, Lt, p, tk, ak, events, nodes, tris, root, eta);
+        if (!(T(0) < thr)) continue;
+        contrib++;
+        T dadw = dAdw<T>(Lt, get_vertex<T>(0, tk, prm) - Lt, p, tk, ak, events, eta);
+        T cosv = std::fmax(dot(normalize(get_vertex<T>(K - 1, tk, prm) - p), n), T(0));
+        T c = thr * (T)lightIntensity / dadw * cosv;
+        c = std::fmin(c, (T)radianceClamp);
+        const float cf = (float)c;
+        const F3 xyz = mk(cmf_x(lambda) / kIntegralCmfY, cmf_y(lambda) / kIntegralCmfY, cmf_z(lambda) / kIntegralCmfY);
+        const F3 Lr = (R / kPi) * xyz2srgblinear(xyz) * cf / p_lambda;
+        float* a = accum + 4 * (size_t)px;
+#pragma omp atomic
+        a[0] += Lr.x;
+#pragma omp atomic
+        a[1] += Lr.y;
+#pragma omp atomic
+        a[2] += Lr.z;
+    }
+    stats[0] = nPairs;
+    stats[1] = conv;
+    stats[2] = contrib;
+}
 // Per-path contributions (before the clamp; 0 = rejected) of every (pair, bin), for the
 // finite-difference references of the adjoint: the set of accepted paths can then be held
 // fixed across the perturbed renders.
@@ -517,6 +569,83 @@ int pzo_render_pairs(int K, int dtype, const int32_t* pairs, int64_t nPairs, con
         default: return -1;
     }
 #undef PZO_R
+}
+
+int pzo_render_pairs_rgb(int K, int dtype, const int32_t* pairs, int64_t nPairs, const int32_t* slotTris,
+                         const float* slotParams, const float* firstDiffuse, const InternalNode* nodes, uint32_t root,
+                         const Triangle* tris, const TriangleAttrib* attribs, const float* p_light,
+                         float lightIntensity, float radianceClamp, uint32_t events, float cauchyA, float cauchyB,
+                         int maxIter, float tol, int warmup, float* accum, int64_t* stats)
+{
+    F3 L = ld3(p_light);
+#define PZO_RGB(KK)                                                                                                  \
+    case KK:                                                                                                         \
+        if (dtype == 0)                                                                                              \
+            render_pairs_rgb<float, KK>(pairs, nPairs, slotTris, slotParams, firstDiffuse, nodes, root, tris,        \
+                                        attribs, L, lightIntensity, radianceClamp, events, cauchyA, cauchyB,        \
+                                        maxIter, tol, warmup, accum, stats);                                        \
+        else                                                                                                         \
+            render_pairs_rgb<double, KK>(pairs, nPairs, slotTris, slotParams, firstDiffuse, nodes, root, tris,       \
+                                         attribs, L, lightIntensity, radianceClamp, events, cauchyA, cauchyB,       \
+                                         maxIter, tol, warmup, accum, stats);                                       \
+        return 0;
+    switch (K) {
+        PZO_RGB(1)
+        PZO_RGB(2)
+        PZO_RGB(3)
+        PZO_RGB(4)
+        default: return -1;
+    }
+#undef PZO_RGB
+}
+
+// CIE 2015 10-degree CMFs and the wavelength sampling (pk.h:960-1012): 0 x, 1 y, 2 z,
+// 3 pdf of the CMF-y logistic, 4 its inverse CDF.
+float pzo_cmf(int which, float nm)
+{
+    switch (which) {
+        case 0: return cmf_x(nm);
+        case 1: return cmf_y(nm);
+        case 2: return cmf_z(nm);
+        case 3: return cmf_y_pdf(nm);
+        case 4: return cmf_y_sample(nm);
+    }
+    return 0.0f;
+}
+
+// pack (main_gpu.cu:499-513): accumulator / count -> sRGB OETF -> RGBA8.
+void pzo_pack(const float* accum, int n, uint32_t* pixels)
+{
+    for (int i = 0; i < n; i++) {
+        const float* a = accum + 4 * (size_t)i;
+        pixels[i] = pack_rgba(srgb_oetf(a[0] / a[3]), srgb_oetf(a[1] / a[3]), srgb_oetf(a[2] / a[3]), 1.0f);
+    }
+}
+
+// Binned spectral image -> linear sRGB and RGBA8: (albedo / pi) * sum_b S_b * srgb(lambda_b)
+// * dlambda, lambda_b the bin centres (the quadrature of the reference's Monte Carlo estimate
+// (R / pi) srgb(lambda) contrib / p(lambda), main_gpu.cu:473-478).  No reference counterpart.
+void pzo_resolve_spectral(const float* spectral, int n, int nBins, float lambdaMin, float lambdaMax,
+                          const float* albedo3, float* rgb4, uint32_t* pixels)
+{
+    const float w = (lambdaMax - lambdaMin) / (float)nBins;
+    const F3 albedo = ld3(albedo3);
+    for (int i = 0; i < n; i++) {
+        F3 c = mk(0.f, 0.f, 0.f);
+        for (int b = 0; b < nBins; b++) {
+            const float lam = lambdaMin + ((float)b + 0.5f) * w;
+            const F3 xyz = mk(cmf_x(lam) / kIntegralCmfY, cmf_y(lam) / kIntegralCmfY, cmf_z(lam) / kIntegralCmfY);
+            c = c + xyz2srgblinear(xyz) * (spectral[(size_t)i * nBins + b] * w);
+        }
+        c = (albedo / kPi) * c;
+        if (rgb4) {
+            rgb4[4 * (size_t)i + 0] = c.x;
+            rgb4[4 * (size_t)i + 1] = c.y;
+            rgb4[4 * (size_t)i + 2] = c.z;
+            rgb4[4 * (size_t)i + 3] = 1.0f;
+        }
+        if (pixels) pixels[i] = pack_rgba(srgb_oetf(c.x), srgb_oetf(c.y), srgb_oetf(c.z), 1.0f);
+    }
 }
 
 int pzo_render_each(int K, int dtype, const int32_t* pairs, int64_t nPairs, const int32_t* slotTris,

@@ -500,3 +500,90 @@ extern "C" int pzr_render_pairs(int K, const int32_t* pairs, int64_t nPairs, con
     return -1;
 }
 
+
+// The reference's own solve mode on the CPU: solveSpecularPath<K> (main_gpu.cu:418-483)
+// written as a loop over the work list around the reference's functions -- eta from the
+// pixel's sampled wavelength (CauchyDispersion), solveConstraints, contributableThroughput,
+// dAdw, the CMF weights (CIE_2015_10deg, xyz2srgblinear) and the wavelength pdf -- adding
+// RGB into a float4 accumulator per pixel (w untouched).
+template <int K>
+static void renderRgbK(const int32_t* pairs, int64_t nPairs, const int32_t* slotTris, const float* slotParams,
+                       const float* fdv, const InternalNode* nodes, uint32_t rootU, const Triangle* tris,
+                       const TriangleAttrib* attribs, float3 L, float I, float clampV, uint32_t ev,
+                       CauchyDispersion cauchy, int maxIter, float tol, int warmup, float* accum, int64_t* stats)
+{
+    EventDescriptor e;
+    e.m_events = ev & 0xFFFFFF;
+    e.m_size = ev >> 24;
+    NodeIndex root = u32Node(rootU);
+    int64_t conv = 0, contrib = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : conv, contrib)
+    for (int64_t q = 0; q < nPairs; q++) {
+        int px = pairs[2 * q], slot = pairs[2 * q + 1];
+        const float* fd = fdv + 10 * (size_t)px;
+        float3 p = ld3(fd), n = ld3(fd + 3), R = ld3(fd + 6);
+        float lambda = fd[9];
+        Triangle tk[K];
+        TriangleAttrib ak[K];
+        for (int k = 0; k < K; k++) { tk[k] = tris[slotTris[4 * slot + k]]; ak[k] = attribs[slotTris[4 * slot + k]]; }
+        float prm[2 * K];
+        for (int i = 0; i < 2 * K; i++) prm[i] = slotParams[8 * slot + i];
+        float p_lambda = CIE_2015_10deg::cmf_y_pdf(lambda);
+        float eta = cauchy(lambda);
+        if (!solveConstraints<K>(prm, L, p, tk, ak, eta, e, maxIter, tol, warmup)) continue;
+        conv++;
+        float thr = contributableThroughput<K>(prm, L, p, tk, ak, e, nodes, tris, root, eta);
+        if (!(0.0f < thr)) continue;
+        contrib++;
+        float dadw = dAdw(L, getVertex(0, tk, prm) - L, p, tk, ak, e, eta);
+        float c = thr * I / dadw * fmaxf(dot(normalize(getVertex(K - 1, tk, prm) - p), n), 0.0f);
+        c = fminf(c, clampV);
+        float3 xyz = {CIE_2015_10deg::cmf_x(lambda) / INTEGRAL_OF_CMF_Y_IN_NM,
+                      CIE_2015_10deg::cmf_y(lambda) / INTEGRAL_OF_CMF_Y_IN_NM,
+                      CIE_2015_10deg::cmf_z(lambda) / INTEGRAL_OF_CMF_Y_IN_NM};
+        float3 srgblinear = xyz2srgblinear(xyz);
+        float3 Lr = (R / PI) * srgblinear * c / p_lambda;
+        float* a = accum + 4 * (size_t)px;
+#pragma omp atomic
+        a[0] += Lr.x;
+#pragma omp atomic
+        a[1] += Lr.y;
+#pragma omp atomic
+        a[2] += Lr.z;
+    }
+    stats[0] = nPairs;
+    stats[1] = conv;
+    stats[2] = contrib;
+}
+extern "C" int pzr_render_pairs_rgb(int K, const int32_t* pairs, int64_t nPairs, const int32_t* slotTris,
+                                    const float* slotParams, const float* fd, const InternalNode* nodes, uint32_t root,
+                                    const Triangle* tris, const TriangleAttrib* attribs, const float* p_light, float I,
+                                    float clampV, uint32_t ev, float cauchyA, float cauchyB, int maxIter, float tol,
+                                    int warmup, float* accum, int64_t* stats)
+{
+    float3 L = ld3(p_light);
+    CauchyDispersion c(cauchyA, cauchyB);
+    switch (K) {
+        case 1: renderRgbK<1>(pairs, nPairs, slotTris, slotParams, fd, nodes, root, tris, attribs, L, I, clampV, ev, c, maxIter, tol, warmup, accum, stats); return 0;
+        case 2: renderRgbK<2>(pairs, nPairs, slotTris, slotParams, fd, nodes, root, tris, attribs, L, I, clampV, ev, c, maxIter, tol, warmup, accum, stats); return 0;
+        case 3: renderRgbK<3>(pairs, nPairs, slotTris, slotParams, fd, nodes, root, tris, attribs, L, I, clampV, ev, c, maxIter, tol, warmup, accum, stats); return 0;
+        case 4: renderRgbK<4>(pairs, nPairs, slotTris, slotParams, fd, nodes, root, tris, attribs, L, I, clampV, ev, c, maxIter, tol, warmup, accum, stats); return 0;
+    }
+    return -1;
+}
+
+// pack (main_gpu.cu:499-513) with the reference's srgb_oetf (pk.h:1023-1031); packRGBA
+// (main_gpu.cu:9-14, device-only in the reference) is the 8-bit quantisation
+// min(max(int(c * 255 + 0.5), 0), 255) per channel, truncating toward zero.
+extern "C" void pzr_pack(const float* accum, int n, uint32_t* pixels)
+{
+    for (int i = 0; i < n; i++) {
+        const float* a = accum + 4 * (size_t)i;
+        int q[3];
+        for (int c = 0; c < 3; c++) {
+            const int v = (int)(srgb_oetf(a[c] / a[3]) * 255.0f + 0.5f);
+            q[c] = v < 0 ? 0 : (v > 255 ? 255 : v);
+        }
+        pixels[i] = 0xFF000000u | ((uint32_t)q[2] << 16) | ((uint32_t)q[1] << 8) | (uint32_t)q[0];
+    }
+}

@@ -54,8 +54,8 @@ class SolveDesc(C.Structure):
                 ("cache_capacity", u32), ("cell_step", f32), ("p_light", Float3), ("light_intensity", f32),
                 ("radiance_clamp", f32), ("cauchy_a", f32), ("cauchy_b", f32), ("accum", vp), ("spectral", vp),
                 ("etas", vp), ("n_bins", i32), ("max_iterations", i32), ("cost_tolerance", f32),
-                ("early_term_warmup", i32), ("stats", vp), ("exact_arithmetic", i32), ("polish_det", f32),
-                ("continuation", i32), ("fold_det", f32), ("graze_cos", f32)]
+                ("early_term_warmup", i32), ("stats", vp), ("fma_contraction", i32), ("polish_det", f32),
+                ("continuation", i32), ("fold_det", f32), ("graze_cos", f32), ("roots", vp)]
 
 
 def f3(v) -> Float3:
@@ -86,6 +86,7 @@ SIGNATURES = {
     "pz_lookup_flatten": (i32, [u32, vp, vp, vp, u32, vp, i32, vp, u32, f32, vp]),
     "pz_reorder_specular_paths": (i32, [vp, vp, vp, u32, vp]),
     "pz_solve_specular_plain": (i32, [C.POINTER(SolveDesc), vp]),
+    "pz_solve_constraints": (i32, [i32, u32, Float3, vp, vp, vp, u32, vp, vp, i32, f32, i32, vp, vp, vp, vp]),
     "pz_solve_batched_scratch_bytes": (sz, [i32, u64]),
     "pz_solve_specular_batched": (i32, [C.POINTER(SolveDesc), vp, vp, sz, i32, vp]),
     "pz_solve_multi_scratch_bytes": (sz, [i32, u32, u64]),

@@ -266,10 +266,11 @@ def sort_and_reorder(frame: Frame, n_paths: int, sorter: OnesweepSort, stream=No
 
 
 def solve_desc(ds: DeviceScene, frame: Frame, cache: PathCache, events_str: str, n_paths: int, spectral=None,
-               etas=None, stats=None, max_iterations=32, cost_tolerance=1e-10, early_term_warmup=1, exact=False,
-               polish_det=0.0, continuation=False, fold_det=0.0, iteration=None, graze_cos=0.0):
+               etas=None, stats=None, max_iterations=32, cost_tolerance=1e-10, early_term_warmup=1, exact=True,
+               polish_det=0.0, continuation=False, fold_det=0.0, iteration=None, graze_cos=0.0, roots=None):
     """Solve descriptor of one event string; the light is the point of `iteration`
-    (Scene.light_point), by default the iteration of the frame's last eye pass."""
+    (Scene.light_point), by default the iteration of the frame's last eye pass.  The plain
+    solve runs without FMA contraction unless exact=False (pz_solve_desc.fma_contraction)."""
     from .scenes import event_descriptor
     sc = ds.scene
     if iteration is None:
@@ -300,11 +301,12 @@ def solve_desc(ds: DeviceScene, frame: Frame, cache: PathCache, events_str: str,
     d.cost_tolerance = cost_tolerance
     d.early_term_warmup = early_term_warmup
     d.stats = stats.data_ptr() if stats is not None else None
-    d.exact_arithmetic = 1 if exact else 0
+    d.fma_contraction = 0 if exact else 1
     d.polish_det = polish_det
     d.continuation = 1 if continuation else 0
     d.fold_det = fold_det
     d.graze_cos = graze_cos
+    d.roots = roots.data_ptr() if roots is not None else None
     return d
 
 

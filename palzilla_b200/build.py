@@ -43,6 +43,7 @@ UNITS = {
     "pz_pathcuts": ("pz_pathcuts.cu", ["-fmad=false"]),
     "pz_adjoint": ("pz_adjoint.cu", ["-fmad=false"]),
     "pz_subdiv": ("pz_subdiv.cu", ["-fmad=false"]),
+    "pz_solve_device": ("pz_solve_device.cu", ["-fmad=false"]),
 }
 
 
@@ -71,7 +72,8 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
     os.makedirs(OBJ, exist_ok=True)
     extra = os.environ.get("PZ_EXTRA_NVCC_FLAGS", "").split()
     headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + \
-        glob.glob(os.path.join(ROOT, "include", "*.h")) + [_stamp_flags(extra)]
+        glob.glob(os.path.join(ROOT, "include", "*.h")) + glob.glob(os.path.join(ROOT, "include", "*.cuh")) + \
+        [_stamp_flags(extra)]
     objs, procs = [], []
     for unit, (srcname, flags) in UNITS.items():
         src = os.path.join(CSRC, srcname)

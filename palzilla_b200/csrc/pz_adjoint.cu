@@ -570,11 +570,11 @@ static cudaError_t launch_adjoint_compact(const adjoint::AdjArgs& a, adjoint::Ad
 {
     const uint64_t items = a.s.nPaths * (uint64_t)a.s.nBins;
     if (items == 0) return cudaSuccess;
-    const unsigned grid = (unsigned)std::min<uint64_t>((items + 255) / 256, (uint64_t)kNumSMs * 32);
+    const unsigned grid = (unsigned)std::min<uint64_t>((items + 255) / 256, (uint64_t)num_sms() * 32);
     adjoint::k_adjoint_filter<K><<<grid, 256, 0, s>>>(a, list, count, capacity, status);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    adjoint::k_adjoint_grad<K><<<kNumSMs * 16, 128, 0, s>>>(a, list, count, capacity);
+    adjoint::k_adjoint_grad<K><<<num_sms() * 16, 128, 0, s>>>(a, list, count, capacity);
     return cudaGetLastError();
 }
 

@@ -53,7 +53,8 @@ constexpr float kProbeTol = 1.0e-3f;  // a plain-solve root farther than this fr
 template <int K> struct PairRec {
     int pixel, slot, mode;  // mode 1: predicted roots, 2: plain per-bin solves
     int polish;             // the item is ill-conditioned: FP64 polish of its roots
-    int scene, pad;         // the item's scene in a batch of scenes
+    int scene;              // the item's scene in a batch of scenes
+    int item;               // the item's index in its scene's work list
     unsigned long long mask;  // bins to solve (mode 1)
     unsigned long long warm;  // of those, bins whose root is deep inside: refine the prediction
     float xa[2 * K], xc[2 * K], xb[2 * K];  // roots at the first, centre and last bin
@@ -464,6 +465,7 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
         r.pixel = sp.pixel;
         r.slot = sp.cacheIndex;
         r.scene = (int)R.scene;
+        r.item = (int)R.local;
         r.mode = 2;
         r.polish = 0;
         r.mask = 0;
@@ -669,6 +671,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
                 const bool conv = newton_nl<K>(xs, ch, S.p_light, fd.p, eta, S.events, S.maxIterations,
                                                S.costTolerance, S.earlyTermWarmUp, true, warm ? 1 : 0, &det);
                 cNewton++;
+                if (conv && S.roots) {
+                    float* rt = S.roots + ((size_t)r.item * B + b) * 8;
+#pragma unroll
+                    for (int i = 0; i < 2 * K; i++) rt[i] = xs[i];
+                }
                 if (conv) {
                     nConv++;
                     const bool polish = r.polish || (double)det < a.polishDet ||
@@ -758,13 +765,13 @@ template <int K>
 static cudaError_t launch_k(const BatchArgs& a, int blocksPerSM, cudaStream_t s, int p1BlocksPerSM = 8)
 {
     if (a.scenes) {
-        k_probe<K, true><<<kNumSMs * 2 * p1BlocksPerSM, 256, 0, s>>>(a);
-        k_phase1<K, true><<<kNumSMs * p1BlocksPerSM, 256, 0, s>>>(a);
-        k_phase2<K, true><<<kNumSMs * blocksPerSM, kWarpsPerBlock * 32, 0, s>>>(a);
+        k_probe<K, true><<<num_sms() * 2 * p1BlocksPerSM, 256, 0, s>>>(a);
+        k_phase1<K, true><<<num_sms() * p1BlocksPerSM, 256, 0, s>>>(a);
+        k_phase2<K, true><<<num_sms() * blocksPerSM, kWarpsPerBlock * 32, 0, s>>>(a);
     } else {
-        k_probe<K, false><<<kNumSMs * 2 * p1BlocksPerSM, 256, 0, s>>>(a);
-        k_phase1<K, false><<<kNumSMs * p1BlocksPerSM, 256, 0, s>>>(a);
-        k_phase2<K, false><<<kNumSMs * blocksPerSM, kWarpsPerBlock * 32, 0, s>>>(a);
+        k_probe<K, false><<<num_sms() * 2 * p1BlocksPerSM, 256, 0, s>>>(a);
+        k_phase1<K, false><<<num_sms() * p1BlocksPerSM, 256, 0, s>>>(a);
+        k_phase2<K, false><<<num_sms() * blocksPerSM, kWarpsPerBlock * 32, 0, s>>>(a);
     }
     return cudaGetLastError();
 }

@@ -306,8 +306,8 @@ cudaError_t build(const Tri* tris, uint32_t n, uint32_t opt, Node* nodes, uint32
         k_build<<<1, kBlock, 0, st>>>(nodes, root, tris, 0, nullptr, nullptr, nullptr, nullptr);
         return cudaGetLastError();
     }
-    const int grid = (int)min((uint32_t)(kNumSMs * 8), (n + kBlock - 1) / kBlock);
-    k_scene_aabb<<<kNumSMs * 8, kBlock, 0, st>>>(tris, n, L.s);
+    const int grid = (int)min((uint32_t)(num_sms() * 8), (n + kBlock - 1) / kBlock);
+    k_scene_aabb<<<num_sms() * 8, kBlock, 0, st>>>(tris, n, L.s);
     k_morton_hist<<<grid, kBlock, 0, st>>>(tris, n, opt, L.s, L.keys, L.lookback, (size_t)sort::num_tiles(n) * sort::kRadix);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (stopAfter == Stage::kKeys) return cudaSuccess;

@@ -209,6 +209,7 @@ int solve_args_from_desc(const pz_solve_desc* d, SolveArgs* a, const char* who)
     a->costTolerance = d->cost_tolerance > 0.0f ? d->cost_tolerance : 1.0e-10f;
     a->earlyTermWarmUp = d->early_term_warmup;
     a->stats = d->stats;
+    a->roots = d->roots;
     return PZ_OK;
 }
 }  // namespace pz
@@ -218,7 +219,7 @@ extern "C" int pz_solve_specular_plain(const pz_solve_desc* desc, pz_stream_t st
     SolveArgs a;
     int r = solve_args_from_desc(desc, &a, "pz_solve_specular_plain");
     if (r != PZ_OK) return r;
-    auto launch = desc->exact_arithmetic ? launch_solve_plain_exact : launch_solve_plain;
+    auto launch = desc->fma_contraction ? launch_solve_plain : launch_solve_plain_exact;
     return done(launch(desc->K, desc->spectral != nullptr, a, S(stream)), "pz_solve_specular_plain");
 }
 

@@ -10,6 +10,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "../../include/palzilla_b200.h"
 
 #define PZ_HD __host__ __device__ __forceinline__
@@ -20,7 +22,36 @@ namespace pz {
 constexpr float kFltMax = 3.402823466e+38F;
 constexpr float kPi = 3.14159265358979323846f;
 constexpr uint32_t kInvalidNode = 0x7FFFFFFFu;
-constexpr int kNumSMs = 148;
+constexpr int kMaxDevices = 64;
+
+// SM count of the current device, looked up once per device ordinal: persistent and
+// grid-stride launches are sized in multiples of it (148 on a B200).
+inline int num_sms()
+{
+    static std::atomic<int> cache[kMaxDevices];  // 0 = not looked up yet
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 148;
+    int v = cache[dev].load(std::memory_order_relaxed);
+    if (v <= 0) {
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+        cache[dev].store(v, std::memory_order_relaxed);
+    }
+    return v;
+}
+
+// Once per (kernel, device) flag for host set-up such as cudaFuncSetAttribute, whose
+// effect is per device: the caller passes a kMaxDevices array owned by the kernel.
+inline bool first_on_device(std::atomic<bool> (&done)[kMaxDevices])
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return true;
+    return !done[dev].load(std::memory_order_acquire);
+}
+inline void mark_done_on_device(std::atomic<bool> (&done)[kMaxDevices])
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxDevices) done[dev].store(true, std::memory_order_release);
+}
 
 struct Tri { float3 v0, v1, v2; };                        // 36 B, minimum_lbvh.h:207
 struct Attrib { int32_t material; float3 n0, n1, n2; };   // 40 B, pk.h:74

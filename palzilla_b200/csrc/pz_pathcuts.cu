@@ -508,7 +508,7 @@ extern "C" size_t pz_path_cuts_scratch_bytes(int K, uint32_t frontier_capacity)
 template <int K>
 static cudaError_t launch_round(const CutArgs& a, int directed, cudaStream_t s)
 {
-    const int grid = kNumSMs * 8;
+    const int grid = num_sms() * 8;
     if (directed) k_cuts_round<K, DR><<<grid, kBlock, 0, s>>>(a);
     else k_cuts_round<K, RN><<<grid, kBlock, 0, s>>>(a);
     return cudaGetLastError();

@@ -64,6 +64,11 @@ __global__ void __launch_bounds__(256) k_solve_plain(SolveArgs a)
     bool conv = solver::solve_constraints<float, K>(prm, L, p, ch, eta, a.events, a.maxIterations, a.costTolerance,
                                                     a.earlyTermWarmUp);
     bool contributing = false;
+    if (conv && a.roots) {
+        float* r = a.roots + (pathIdx * nb + bin) * 8;
+#pragma unroll
+        for (int i = 0; i < 2 * K; i++) r[i] = prm[i];
+    }
     if (conv) {
         const float thr = solver::contributable_throughput<float, K>(prm, L, p, ch, a.events, a.nodes, a.tris, root, eta);
         if (0.0f < thr) {

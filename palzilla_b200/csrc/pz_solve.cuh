@@ -26,6 +26,7 @@ struct SolveArgs {
     float costTolerance;       // 1e-10
     int earlyTermWarmUp;       // 1
     unsigned long long* stats; // [solves, converged, contributing] or null
+    float* roots;              // converged roots, 8 floats per (item, bin), or null
 };
 
 cudaError_t launch_solve_plain(int K, bool binned, const SolveArgs& a, cudaStream_t s);

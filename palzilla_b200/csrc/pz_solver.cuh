@@ -109,6 +109,24 @@ PZ_D void load_chain(Chain<K>& c, const Tri* __restrict__ tris, const Attrib* __
     }
 }
 
+// The chain of triangles and attributes given by value (the reference's solver arguments).
+template <int K>
+PZ_D void make_chain(Chain<K>& c, const Tri* tris, const Attrib* attribs)
+{
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        const float3 a = tris[k].v0, b = tris[k].v1, d = tris[k].v2;
+        c.v0[k] = a;
+        c.e0[k] = b - a;
+        c.e1[k] = d - a;
+        c.ng[k] = cross(b - a, d - a);
+        c.n0[k] = attribs[k].n0;
+        c.ne0[k] = attribs[k].n1 - attribs[k].n0;
+        c.ne1[k] = attribs[k].n2 - attribs[k].n0;
+        c.material[k] = attribs[k].material;
+    }
+}
+
 // ---------------------------------------------------------------- Householder QR least squares
 // Solves min |A x - b| for A (R x C, column-major, R >= C) by the reference's
 // Householder construction (sen.h:658-747).
@@ -164,9 +182,17 @@ PZ_D void qr_solve(T (&A)[C][R], T (&b)[R], T (&x)[C])
 }
 
 // ---------------------------------------------------------------- Newton solve
-template <class T, int K>
+// The end-of-iteration callback of solveConstraints (pk.h:461-463): called with
+// (iteration, true) when the cost test passes, and with (iteration, iteration ==
+// maxIterations - 1) after every other iteration that is not rejected at a triangle edge.
+struct NoCallback {
+    PZ_D void operator()(int, bool) const {}
+};
+
+template <class T, int K, class Callback = NoCallback>
 PZ_D bool solve_constraints(T* params, V3<T> p_beg, V3<T> p_end, const Chain<K>& ch, T eta, uint32_t events,
-                            int maxIterations, T costTolerance, int earlyTermWarmUp, int* itersOut = nullptr)
+                            int maxIterations, T costTolerance, int earlyTermWarmUp, int* itersOut = nullptr,
+                            Callback end_of_iter = Callback())
 {
     constexpr int NP = 2 * K;
     T edge_eps = T(0.25);
@@ -210,6 +236,7 @@ PZ_D bool solve_constraints(T* params, V3<T> p_beg, V3<T> p_end, const Chain<K>&
         }
         if (cost < costTolerance) {
             if (itersOut) *itersOut = iter;
+            end_of_iter(iter, true);
             return true;
         }
         T dp[NP];
@@ -227,6 +254,7 @@ PZ_D bool solve_constraints(T* params, V3<T> p_beg, V3<T> p_end, const Chain<K>&
             }
             edge_eps *= edge_eps;
         }
+        end_of_iter(iter, iter == maxIterations - 1);
     }
     if (itersOut) *itersOut = maxIterations;
     return false;

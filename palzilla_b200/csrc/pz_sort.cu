@@ -293,7 +293,7 @@ template <class KeyT>
 cudaError_t launch_hist(const KeyT* keys, uint32_t n, int startBit, int nPasses, Header* h,
                         unsigned long long* lookback, cudaStream_t s)
 {
-    int blocks = kNumSMs * kHistBlocksPerSM;
+    int blocks = num_sms() * kHistBlocksPerSM;
     uint32_t need = (n + kThreads * 8 - 1) / (kThreads * 8);
     if ((uint32_t)blocks > need) blocks = (int)(need > 0 ? need : 1);
     k_hist<KeyT><<<blocks, kThreads, 0, s>>>(keys, n, startBit, nPasses, h, lookback,
@@ -306,12 +306,13 @@ static cudaError_t launch_pass(const KeyT* kin, KeyT* kout, const uint32_t* vin,
                                int pass, Header* h, unsigned long long* lookback, cudaStream_t s)
 {
     const size_t smem = sizeof(PassSmem<KeyT, kHasVal>);
-    static bool configured = false;  // the attribute is per function, set once
-    if (!configured) {
+    // the shared-memory limit is an attribute of the function on each device: set it once per device
+    static std::atomic<bool> configured[kMaxDevices];
+    if (first_on_device(configured)) {
         cudaError_t e = cudaFuncSetAttribute(k_pass<KeyT, kHasVal>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;
-        configured = true;
+        mark_done_on_device(configured);
     }
     k_pass<KeyT, kHasVal><<<num_tiles(n), kThreads, smem, s>>>(kin, kout, vin, vout, n, bit, pass, h, lookback);
     return cudaGetLastError();

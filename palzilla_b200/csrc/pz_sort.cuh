@@ -67,6 +67,10 @@ struct Header {
 };
 constexpr size_t kHeaderBytes = 16384;
 static_assert(sizeof(Header) <= kHeaderBytes, "header");
+// The digit stage runs one thread per digit, and warps are whole.
+static_assert(kThreads >= kRadix && kThreads % 32 == 0, "PZ_SORT_THREADS: a multiple of 32, at least 256");
+// Per-item ranks within a tile are kept as uint16.
+static_assert(kTile <= 65536, "PZ_SORT_THREADS * PZ_SORT_ITEMS must not exceed 65536");
 
 inline uint32_t num_tiles(uint32_t n) { return (n + kTile - 1) / kTile; }
 inline int num_passes(int startBit, int endBit) { return (endBit - startBit + 7) / 8; }

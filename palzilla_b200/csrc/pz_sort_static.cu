@@ -2,14 +2,17 @@
 // scratch array, for callers that cannot allocate device memory at call time.
 //
 // The scratch (sort header + look-back rows for PZ_ONESWEEP_STATIC_MAX_KEYS keys) is a
-// __device__ array of this library; its address is looked up once per device with
-// cudaGetSymbolAddress and cached.  The sort itself is pz_onesweep_sort, unchanged, given
-// that array as its scratch.  Nothing in the array has to start at zero: every call clears
-// the header with cudaMemsetAsync on its stream and the histogram kernel clears the
-// look-back rows it uses.  The array is shared by every call on a device, so calls whose
-// work overlaps on the GPU (different streams without ordering) race on it.
-#include <mutex>
-
+// __device__ array of this library.  A __device__ symbol has one address per CUDA context
+// (the module is loaded into each context separately), so every call looks the address up
+// with cudaGetSymbolAddress in the context current on the calling thread: a host that makes
+// its own contexts, or re-creates the primary context after cudaDeviceReset, gets the
+// address that belongs to the context it is running in.  The look-up allocates nothing; the
+// first one in a context may load this library's module into it.  The sort itself is
+// pz_onesweep_sort, unchanged, given that array as its scratch.  Nothing in the array has to
+// start at zero: every call clears the header with cudaMemsetAsync on its stream and the
+// histogram kernel clears the look-back rows it uses.  The array is shared by every call in
+// a context, so calls whose work overlaps on the GPU (different streams without ordering)
+// race on it.
 #include "pz_capi_internal.h"
 #include "pz_sort.cuh"
 
@@ -19,30 +22,17 @@ namespace {
 constexpr uint32_t kStaticMaxKeys = PZ_ONESWEEP_STATIC_MAX_KEYS;
 constexpr size_t kStaticLookback = (size_t)((kStaticMaxKeys + sort::kTile - 1) / sort::kTile) * sort::kRadix * 8;
 constexpr size_t kStaticBytes = sort::kHeaderBytes + ((kStaticLookback + 255) & ~(size_t)255);
-constexpr int kMaxDevices = 64;
 
 __device__ __align__(256) unsigned char g_sort_scratch[kStaticBytes];
 
-std::mutex g_mutex;
-void* g_scratch_ptr[kMaxDevices] = {};
-
-// Device address of g_sort_scratch on the current device (looked up on first use).
+// Device address of g_sort_scratch in the current context.
 int static_scratch(void** out)
 {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return cuda_fail(e, "pz_onesweep_sort_static: cudaGetDevice");
-    if (dev < 0 || dev >= kMaxDevices)
-        return fail(PZ_ERR_UNSUPPORTED, "pz_onesweep_sort_static: device ordinal %d >= %d", dev, kMaxDevices);
-    std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_scratch_ptr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_sort_scratch);
-        if (e != cudaSuccess) return cuda_fail(e, "pz_onesweep_sort_static: cudaGetSymbolAddress");
-        if (!p) return fail(PZ_ERR_CUDA, "pz_onesweep_sort_static: null scratch symbol address");
-        g_scratch_ptr[dev] = p;
-    }
-    *out = g_scratch_ptr[dev];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_sort_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "pz_onesweep_sort_static: cudaGetSymbolAddress");
+    if (!p) return fail(PZ_ERR_CUDA, "pz_onesweep_sort_static: null scratch symbol address");
+    *out = p;
     return PZ_OK;
 }
 

@@ -940,7 +940,7 @@ static cudaError_t sort_leaves(const SubArgs& a, uint64_t* fronts[2], size_t par
 template <int K>
 static cudaError_t run(SubArgs& a, uint64_t* fronts[2], size_t part, unsigned long long* counts, cudaStream_t s)
 {
-    const int grid = kNumSMs * 8;
+    const int grid = num_sms() * 8;
     k_sub_init<<<(a.nRows + kBlock - 1) / kBlock, kBlock, 0, s>>>(a, fronts[0], &counts[0]);
     cudaError_t e = cudaGetLastError();
     int cur = 0;
@@ -1124,7 +1124,7 @@ extern "C" int pz_subdivide_contribute(int K, uint32_t events, pz_float3 p_beg, 
     a.attribs = reinterpret_cast<const Attrib*>(attribs_dev);
     a.spectral = spectral_dev;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const unsigned grid = (unsigned)std::min<uint64_t>((n_roots + kBlock - 1) / kBlock, (uint64_t)kNumSMs * 16);
+    const unsigned grid = (unsigned)std::min<uint64_t>((n_roots + kBlock - 1) / kBlock, (uint64_t)num_sms() * 16);
     switch (K) {
         case 1: k_sub_contribute<1><<<grid, kBlock, 0, s>>>(a); break;
         case 2: k_sub_contribute<2><<<grid, kBlock, 0, s>>>(a); break;

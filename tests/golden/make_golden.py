@@ -12,7 +12,9 @@ rebuild a scene to check the oracle:
 - closest and any hits of seeded rays;
 - photon records and PathCache slots;
 - solveConstraints, contributableThroughput and dAdw on photon tuples;
-- a binned render of a small lens frame;
+- a binned render of a small lens frame, and the same work list in the reference's own
+  per-pixel-wavelength mode (RGB accumulator);
+- CIE 2015 CMF samples, the wavelength pdf and sampling, and pack (RGBA8);
 - interval square / normalize, Fresnel and refraction samples;
 - normal bounds and path-cuts tuple sets (K = 1 lens, K = 2 two-sheet lens).
 """
@@ -104,6 +106,24 @@ def main():
     img, st = ref.render_pairs(1, pairs, cache, fd, lens_bvh, lens, lens.bin_etas())
     g.update(render_fd=fd, render_pairs=pairs, render_etas=lens.bin_etas(), render_spectral=img,
              render_stats=st)
+    # the same work list in the reference's own mode: each pixel's sampled wavelength, RGB into
+    # a float4 accumulator (solveSpecularPath<K>, main_gpu.cu:418-483)
+    acc, st_rgb = ref.render_pairs_rgb(1, pairs, cache, fd, lens_bvh, lens)
+    g.update(render_rgb_accum=acc, render_rgb_stats=st_rgb)
+
+    # ---- spectral model (CIE 2015 10-degree CMFs, wavelength pdf and sampling) and pack
+    nm = np.linspace(360.0, 830.0, 941).astype(np.float32)
+    u = np.linspace(0.0, 1.0, 257).astype(np.float32)
+    g["cmf_nm"] = nm
+    g["cmf_u"] = u
+    g["cmf_out"] = np.stack([ref.cmf(w, nm) for w in range(4)], 0)
+    g["cmf_sample"] = ref.cmf(4, u)
+    rng_pack = np.random.default_rng(23)
+    acc_in = rng_pack.uniform(0.0, 4.0, (512, 4)).astype(np.float32)
+    acc_in[:, 3] = rng_pack.integers(1, 33, 512).astype(np.float32)
+    acc_in[:8, :3] = np.array([0.0, 1e-4, 3.13e-3, 1.0, 2.0, 100.0, 0.5, 0.25], np.float32)[:, None]
+    g["pack_in"] = acc_in
+    g["pack_out"] = ref.pack(acc_in)
 
     # ---- interval arithmetic, Fresnel, refraction
     xs = np.linspace(-16, 16, 257).astype(np.float32)

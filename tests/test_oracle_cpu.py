@@ -108,6 +108,25 @@ def test_binned_render_bitwise(orc, g, lens):
     assert (img > 0).sum() > 100
 
 
+def test_reference_mode_render(orc, g, lens):
+    """The reference's own per-pixel-wavelength solve (main_gpu.cu:418-483) on the golden work
+    list: the same accepted paths, and RGB accumulators equal up to the order of the float adds
+    of a pixel's paths."""
+    acc, st = orc.render_pairs_rgb(1, g["render_pairs"], _full_cache(g), g["render_fd"], _bvh(g, "lens"), lens)
+    assert np.array_equal(st, g["render_rgb_stats"]) and st[2] > 0
+    exp = g["render_rgb_accum"]
+    assert np.allclose(acc, exp, rtol=2e-6, atol=1e-7 * float(np.abs(exp).max()))
+
+
+def test_spectral_model_and_pack_bitwise(orc, g):
+    """CIE 2015 10-degree CMFs, the wavelength pdf and its sampling (pk.h:960-1012) and pack
+    (main_gpu.cu:499-513) equal the reference's bit for bit."""
+    got = np.stack([orc.cmf(w, g["cmf_nm"]) for w in range(4)], 0)
+    assert got.tobytes() == g["cmf_out"].tobytes()
+    assert orc.cmf(4, g["cmf_u"]).tobytes() == g["cmf_sample"].tobytes()
+    assert np.array_equal(orc.pack(g["pack_in"]), g["pack_out"])
+
+
 def test_interval_fresnel_refract_bitwise(orc, g):
     out = np.array([orc.interval_square(l, u) for l, u in g["isq_in"]], np.float32)
     assert out.tobytes() == g["isq_out"].tobytes()

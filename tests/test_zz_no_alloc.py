@@ -1,8 +1,11 @@
 """pz_onesweep_sort_static (sort on the library's static device scratch) against
-pz_onesweep_sort (caller-owned scratch): two different sorts in a row on one stream must
-both match the caller-scratch results bit for bit, and an oversize request is refused
-before any device work.  Collected last, so it also runs after the other GPU tests have
-used the device."""
+pz_onesweep_sort (caller-owned scratch), for callers that cannot allocate device memory:
+two different sorts in a row on one stream must both match the caller-scratch results bit
+for bit; after the first call, further calls must leave the device's free memory
+unchanged; a sort in a second CUDA context (made with the driver API, as a plug-in host
+that owns its context would) must use that context's copy of the array; and an oversize
+request is refused before any device work.  Collected last, so it also runs after the
+other GPU tests have used the device."""
 import ctypes as C
 
 import numpy as np
@@ -79,3 +82,75 @@ def test_static_scratch_rejects_oversize_before_device_work():
     assert b"static scratch capacity" in L.pz_last_error()
     torch.cuda.synchronize()
     assert torch.equal(keys, before)
+
+
+def test_static_scratch_allocates_nothing_after_the_first_call():
+    L = _lib.lib()
+    rng = np.random.default_rng(7)
+    n = 1 << 21
+    keys = rng.integers(0, 1 << 32, n, dtype=np.uint64)
+    k, tk = _dev(keys), torch.empty(n, dtype=torch.int64, device="cuda")
+    s = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert L.pz_onesweep_sort_static(_p(k), None, _p(tk), None, C.c_uint32(n), 8, 0, 32, None, s) == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        k.copy_(_dev(keys))
+        assert L.pz_onesweep_sort_static(_p(k), None, _p(tk), None, C.c_uint32(n), 8, 0, 32, None, s) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    order = np.argsort(keys & np.uint64(0xFFFFFFFF), kind="stable")
+    assert np.array_equal(k.cpu().numpy().view(np.uint64), keys[order])
+
+
+def test_static_scratch_in_a_second_context():
+    """A host that runs the library in a context of its own: the array's address is looked
+    up in that context, not reused from the primary context of the same device."""
+    from cuda.bindings import driver as D
+
+    def ok(r):
+        err = r[0] if isinstance(r, tuple) else r
+        assert err == D.CUresult.CUDA_SUCCESS, err
+        return r[1] if isinstance(r, tuple) and len(r) == 2 else r
+
+    L = _lib.lib()
+    torch.cuda.synchronize()  # the primary context exists and is current
+    n = (1 << 20) + 333
+    keys = np.random.default_rng(11).integers(0, 1 << 32, n, dtype=np.uint64)
+    dev = ok(D.cuDeviceGet(torch.cuda.current_device()))
+    mode = ok(D.cuDeviceGetAttribute(D.CUdevice_attribute.CU_DEVICE_ATTRIBUTE_COMPUTE_MODE, dev))
+    if int(mode) != int(D.CUcomputemode.CU_COMPUTEMODE_DEFAULT):
+        pytest.skip(f"compute mode {mode} allows one context per device")
+    ctx = ok(D.cuCtxCreate(0, dev))
+    bufs = []
+    try:
+        kd = ok(D.cuMemAlloc(8 * n))
+        bufs.append(kd)
+        td = ok(D.cuMemAlloc(8 * n))
+        bufs.append(td)
+        sd = ok(D.cuMemAlloc(4))
+        bufs.append(sd)
+        ok(D.cuMemcpyHtoD(kd, keys.ctypes.data, 8 * n))
+        ok(D.cuMemsetD32(sd, 0xFFFFFFFF, 1))
+        r = L.pz_onesweep_sort_static(C.c_void_p(int(kd)), None, C.c_void_p(int(td)), None, C.c_uint32(n), 8, 0, 32,
+                                      C.c_void_p(int(sd)), None)
+        assert r == 0, L.pz_last_error()
+        ok(D.cuCtxSynchronize())
+        got = np.empty(n, np.uint64)
+        st = np.empty(1, np.uint32)
+        ok(D.cuMemcpyDtoH(got.ctypes.data, kd, 8 * n))
+        ok(D.cuMemcpyDtoH(st.ctypes.data, sd, 4))
+    finally:
+        for b in bufs:
+            D.cuMemFree(b)
+        ok(D.cuCtxDestroy(ctx))
+    order = np.argsort(keys & np.uint64(0xFFFFFFFF), kind="stable")
+    assert int(st[0]) == 0
+    assert np.array_equal(got, keys[order])
+    # the primary context is current again and still sorts on its own copy of the array
+    k, tk = _dev(keys), torch.empty(n, dtype=torch.int64, device="cuda")
+    assert L.pz_onesweep_sort_static(_p(k), None, _p(tk), None, C.c_uint32(n), 8, 0, 32, None,
+                                     C.c_void_p(torch.cuda.current_stream().cuda_stream)) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(k.cpu().numpy().view(np.uint64), keys[order])
