@@ -281,11 +281,12 @@ PZ_API int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32_t* 
  * which are overwritten with the solver's last iterate (the root when it converged).
  * converged_dev[i] (may be NULL) = 1 when the cost tolerance was reached; iters_dev[i] (may
  * be NULL) = the last iteration passed to the end-of-iteration callback (-1 when the solve
- * was rejected at a triangle edge before any callback). */
+ * was rejected at a triangle edge before any callback).  An item whose triangle indices are
+ * not below n_triangles is not solved: converged 0, iteration -2, parameters unchanged. */
 PZ_API int pz_solve_constraints(int K, uint32_t events, pz_float3 p_beg, const int32_t* tuples_dev,
                                 const pz_float3* p_end_dev, const float* etas_dev, uint32_t n,
                                 const pz_triangle* triangles_dev, const pz_triangle_attrib* attribs_dev,
-                                int max_iterations, float cost_tolerance, int early_term_warmup, float* params_dev,
+                                uint32_t n_triangles, int max_iterations, float cost_tolerance, int early_term_warmup, float* params_dev,
                                 uint8_t* converged_dev, int32_t* iters_dev, pz_stream_t stream);
 
 /* ---------------------------------------------------------------- batches of scenes

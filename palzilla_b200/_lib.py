@@ -86,7 +86,7 @@ SIGNATURES = {
     "pz_lookup_flatten": (i32, [u32, vp, vp, vp, u32, vp, i32, vp, u32, f32, vp]),
     "pz_reorder_specular_paths": (i32, [vp, vp, vp, u32, vp]),
     "pz_solve_specular_plain": (i32, [C.POINTER(SolveDesc), vp]),
-    "pz_solve_constraints": (i32, [i32, u32, Float3, vp, vp, vp, u32, vp, vp, i32, f32, i32, vp, vp, vp, vp]),
+    "pz_solve_constraints": (i32, [i32, u32, Float3, vp, vp, vp, u32, vp, vp, u32, i32, f32, i32, vp, vp, vp, vp]),
     "pz_solve_batched_scratch_bytes": (sz, [i32, u64]),
     "pz_solve_specular_batched": (i32, [C.POINTER(SolveDesc), vp, vp, sz, i32, vp]),
     "pz_solve_multi_scratch_bytes": (sz, [i32, u32, u64]),

@@ -16,13 +16,15 @@
 //    converge, whose prediction is strongly nonlinear, or whose Jacobian is near a fold,
 //    take the plain per-bin solve for every bin.  Items with work are appended to a record
 //    list with warp-aggregated atomics;
-//  * k_phase2, persistent, one warp per record and one lane per bin: bins deep inside the
-//    triangles refine the predicted root; every other bin runs the plain path's solve from
-//    the photon's barycentrics, so its accept / reject decision is the plain one.  Then
-//    admissibility, visibility shared by the whole warp (one BVH query per path segment
-//    with the segment fattened to cover every bin's segment; each bin tests only those
-//    candidates), dAdw and the spectral accumulation.  Optional FP64 polish of roots whose
-//    relative Jacobian determinant is below a threshold.
+//  * phase 2, in waves of three kernels (see the phase-2 section): k_p2_solve, one warp per
+//    record, lanes over the record's bins to solve in rank order: bins deep inside the
+//    triangles refine the predicted root, every other bin runs the plain path's solve from
+//    the photon's barycentrics, so its accept / reject decision is the plain one; then
+//    admissibility, with optional FP64 polish of roots whose relative Jacobian determinant is
+//    below a threshold; k_p2_vis, one warp per round of accepted roots of one record:
+//    visibility shared by the warp (one BVH query per path segment with the segment fattened
+//    to cover every root's segment; each root tests only those candidates); k_p2_contrib, one
+//    thread per visible root: dAdw and the spectral accumulation.
 // The unit is compiled without FMA contraction: with the reference's operation order in
 // every Newton step, the image equals the reference's float arithmetic up to the order
 // of the float atomics.
@@ -599,39 +601,78 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
 }
 
 // ---------------------------------------------------------------- phase 2
-template <int K, bool kMulti>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
+// Phase 2 runs in waves of three kernels.  Each wave takes records (phase-1 items with bins
+// to solve) from the work counter while the accepted list has room for 64 more roots per
+// record (a record never has more), so any input fits in a fixed number of waves:
+//  * k_p2_solve, one warp per record: the lanes take the record's bins to solve in rank
+//    order (32 at a time, no lane idles for a bin the mask excludes); Newton, then
+//    admissibility; the accepted (converged and admissible) roots of each round are
+//    appended as one block {first, record, count};
+//  * k_p2_vis, one warp per block: the shadow segments of the block's roots share one
+//    fattened BVH query per path segment (all roots of a block belong to one record, so
+//    their segments are close); a root that is occluded gets throughput 0;
+//  * k_p2_contrib, one thread per accepted root: dAdw and the clamped contribution, added
+//    to the spectral image.
+// Each kernel is a short body at modest register count, where the single phase-2 kernel it
+// replaces held Newton, the queries and dAdw at once (instruction-fetch bound at 25%
+// occupancy, and idle lanes for every bin a record did not solve).
+
+// Accepted root of phase 2.
+template <int K> struct Accepted {
+    uint32_t rec;   // phase-1 record
+    uint32_t bin;   // wavelength bin
+    float thr;      // Fresnel product after admissibility; 0 once occluded
+    float x[2 * K]; // barycentrics of the root
+};
+// Round of accepted roots of one record: entries [first, first + count) of the accepted list.
+struct AcceptBlock {
+    uint32_t first, rec, count;
+};
+
+// The record's bin mask to solve.
+template <int K>
+PZ_D unsigned long long record_todo(const PairRec<K>& r, int B)
 {
-    __shared__ uint32_t cand[kWarpsPerBlock][kMaxCand];
-    __shared__ uint32_t front[kWarpsPerBlock][2 * kFront];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    return r.mode == 2 ? (B == 64 ? ~0ull : ((1ull << B) - 1ull)) : r.mask;
+}
+
+template <int K, bool kMulti>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_p2_solve(BatchArgs a)
+{
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = (1u << lane) - 1u;
     const int B = a.s.nBins;
     const unsigned long long nRec = min(*a.recordCount, a.recordCapacity);
     const auto* recs = reinterpret_cast<const PairRec<K>*>(a.records);
-    const int chunk = a.chunk > 0 ? a.chunk : 1;
-    unsigned long long nConv = 0, nContrib = 0;
-    // diagnostic counts, kept per thread and added once at the end
-    unsigned long long cNewton = 0, cPolish = 0, cQueries = 0, cOverflow = 0, cCand = 0;
-    unsigned long long j = 0, jEnd = 0;
+    auto* acc = reinterpret_cast<Accepted<K>*>(a.accepted);
+    auto* blocks = reinterpret_cast<AcceptBlock*>(a.blocks);
+    unsigned long long* const nAccepted = a.p2 + 0;
+    unsigned long long* const nBlocks = a.p2 + 1;
+    unsigned long long* const reserved = a.p2 + 2;
+    unsigned long long nConv = 0, cNewton = 0, cPolish = 0;
     for (;;) {
-        // the warp takes `chunk` records at a time from the work counter
-        if (j >= jEnd) {
-            if (lane == 0) j = atomicAdd(a.workCounter, (unsigned long long)chunk);
-            j = __shfl_sync(0xFFFFFFFFu, j, 0);
-            jEnd = min(j + (unsigned long long)chunk, nRec);
+        // one record per queue access, after reserving room for its accepted roots in this wave
+        unsigned long long j = 0;
+        bool take = false;
+        if (lane == 0) {
+            if (*a.workCounter < nRec && atomicAdd(reserved, 64ull) + 64ull <= a.acceptCapacity) {
+                j = atomicAdd(a.workCounter, 1ull);
+                take = j < nRec;
+            }
         }
-        if (j >= nRec) break;
-        const PairRec<K> r = recs[j++];
+        take = __shfl_sync(0xFFFFFFFFu, take, 0);
+        if (!take) break;
+        j = __shfl_sync(0xFFFFFFFFu, j, 0);
+        const PairRec<K> r = recs[j];
         const SolveArgs& S = kMulti ? a.scenes[r.scene].s : a.s;
-        const uint32_t root = __ldg(S.root);
         const float eta_c = S.etas[B / 2];
         const V3<float> L = v3f<float>(S.p_light);
         const int4 ti = S.cache.tris[r.slot];
         const int tix[4] = {ti.x, ti.y, ti.z, ti.w};
         Chain<K> ch;
         load_chain<K>(ch, S.tris, S.attribs, tix);
-        const FirstDiffuse fd = S.fds[r.pixel];
-        const V3<float> p = v3f<float>(fd.p);
+        const float3 pe = S.fds[r.pixel].p;
+        const V3<float> p = v3f<float>(pe);
         float x0[2 * K];
         {
             const float4 q0 = S.cache.params[2 * r.slot], q1 = S.cache.params[2 * r.slot + 1];
@@ -639,23 +680,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
 #pragma unroll
             for (int i = 0; i < 2 * K; i++) x0[i] = pp[i];
         }
-        // lanes take the bins to solve in rank order (the set bits of the item's mask)
-        const unsigned long long todo = r.mode == 2 ? (B == 64 ? ~0ull : ((1ull << B) - 1ull)) : r.mask;
-#if PZ_BATCHED_RANK
+        const unsigned long long todo = record_todo<K>(r, B);
         const int nTodo = __popcll(todo);
         for (int round = 0; round * 32 < nTodo; round++) {
             const int rank = lane + 32 * round;
             const int b = rank < nTodo ? nth_bit64(todo, rank) : B;
-#else
-        for (int round = 0; round * 32 < B; round++) {
-            const int b0 = lane + 32 * round;
-            const int b = (b0 < B && ((todo >> b0) & 1ull)) ? b0 : B;
-#endif
             float xs[2 * K];
             float thr = 0.0f;
-            // the chain's vertices and shading normals as the admissibility test built them:
-            // the endpoints of the shadow segments (contributableThroughput, pk.h:763-827)
-            float3 vtx[K + 2], nrm[K + 2];
             if (b < B) {
                 const float eta = S.etas[b];
                 const bool warm = r.mode == 1 && (a.continuation || ((r.warm >> b) & 1ull));
@@ -668,7 +699,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
                 float det = 1.0f;
                 // a predicted root is refined by Newton; every other bin runs the plain path's
                 // solver from the photon's start, so its accept / reject decision is the plain one
-                const bool conv = newton_nl<K>(xs, ch, S.p_light, fd.p, eta, S.events, S.maxIterations,
+                const bool conv = newton_nl<K>(xs, ch, S.p_light, pe, eta, S.events, S.maxIterations,
                                                S.costTolerance, S.earlyTermWarmUp, true, warm ? 1 : 0, &det);
                 cNewton++;
                 if (conv && S.roots) {
@@ -679,101 +710,197 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_phase2(BatchArgs a)
                 if (conv) {
                     nConv++;
                     const bool polish = r.polish || (double)det < a.polishDet ||
-                                        (a.grazeCos > 0.0f && min_abs_cos<K>(ch, xs, S.p_light, fd.p) < a.grazeCos);
+                                        (a.grazeCos > 0.0f && min_abs_cos<K>(ch, xs, S.p_light, pe) < a.grazeCos);
                     cPolish += polish;
+                    float3 vtx[K + 2], nrm[K + 2];
                     if (polish)
-                        thr = polish_fp64<K>(xs, ch, S.p_light, fd.p, S.events, eta, vtx, nrm);
+                        thr = polish_fp64<K>(xs, ch, S.p_light, pe, S.events, eta, vtx, nrm);
                     else
                         thr = pre_throughput<float, K>(xs, L, p, ch, S.events, eta, vtx, nrm);
                 }
             }
-            // shared visibility: one fattened query per segment for all bins of the round
-            for (int s = 0; s < K + 1; s++) {
-                const uint32_t valid = __ballot_sync(0xFFFFFFFFu, thr > 0.0f);
-                if (!valid) break;
-                const int leader = __ffs(valid) - 1;
-                float3 sa = mk3(0.f, 0.f, 0.f), sb = mk3(0.f, 0.f, 0.f);
-                if (thr > 0.0f) {
-                    shadow_segment(pick<K + 2>(vtx, s), pick<K + 2>(nrm, s), pick<K + 2>(vtx, s + 1),
-                                   pick<K + 2>(nrm, s + 1), sa, sb);
-                }
-                const float3 ra = mk3(__shfl_sync(0xFFFFFFFFu, sa.x, leader), __shfl_sync(0xFFFFFFFFu, sa.y, leader),
-                                      __shfl_sync(0xFFFFFFFFu, sa.z, leader));
-                const float3 rb = mk3(__shfl_sync(0xFFFFFFFFu, sb.x, leader), __shfl_sync(0xFFFFFFFFu, sb.y, leader),
-                                      __shfl_sync(0xFFFFFFFFu, sb.z, leader));
-                float rad = 0.0f, mag = 0.0f;
-                if (thr > 0.0f) {
-                    const float3 da = vabs(sa - ra), db = vabs(sb - rb);
-                    rad = fmaxf(fmaxf(fmaxf(da.x, da.y), da.z), fmaxf(fmaxf(db.x, db.y), db.z));
-                    const float3 ma = vabs(sa), mb = vabs(sb);
-                    mag = fmaxf(fmaxf(fmaxf(ma.x, ma.y), ma.z), fmaxf(fmaxf(mb.x, mb.y), mb.z));
-                }
-                rad = warp_max(rad);
-                mag = warp_max(mag);
-                rad += 1.0e-5f * (1.0f + mag);  // covers the rounding of the slab and box arithmetic
-                const int nc = fat_query(S.nodes, root, ra, rb, rad, cand[warp], front[warp]);
-                __syncwarp();
+            // this round's accepted roots: one block of consecutive entries
+            const uint32_t ok = __ballot_sync(0xFFFFFFFFu, thr > 0.0f);
+            if (ok) {
+                unsigned long long first = 0;
                 if (lane == 0) {
-                    cQueries++;
-                    if (nc < 0) cOverflow++;
-                    else cCand += (unsigned long long)nc;
+                    first = atomicAdd(nAccepted, (unsigned long long)__popc(ok));
+                    const unsigned long long bi = atomicAdd(nBlocks, 1ull);
+                    if (bi < a.blockCapacity && first + __popc(ok) <= a.acceptCapacity)
+                        blocks[bi] = AcceptBlock{(uint32_t)first, (uint32_t)j, (uint32_t)__popc(ok)};
+                    else
+                        raise_error(a.status, kErrCapacity);  // cannot happen: room was reserved
                 }
-                if (thr > 0.0f) {
-                    const float3 d = ex::sub3(sb, sa);
-                    bool occ = false;
-                    if (nc < 0) {
-                        occ = any_hit(S.nodes, S.tris, root, sa, d, 1.0f) < 1.0f;
-                    } else {
-                        for (int c = 0; c < nc && !occ; c++) {
-                            float3 v0, v1, v2;
-                            load_tri(S.tris, cand[warp][c], v0, v1, v2);
-                            float t, u, v;
-                            float3 ng;
-                            if (ray_triangle(&t, &u, &v, &ng, 0.0f, 1.0f, sa, d, v0, v1, v2) && t < 1.0f) occ = true;
-                        }
-                    }
-                    if (occ) thr = 0.0f;
+                first = __shfl_sync(0xFFFFFFFFu, first, 0);
+                const unsigned long long dst = first + __popc(ok & lt);
+                if (thr > 0.0f && dst < a.acceptCapacity) {
+                    Accepted<K> e;
+                    e.rec = (uint32_t)j;
+                    e.bin = (uint32_t)b;
+                    e.thr = thr;
+#pragma unroll
+                    for (int i = 0; i < 2 * K; i++) e.x[i] = xs[i];
+                    acc[dst] = e;
                 }
-                __syncwarp();
-            }
-            if (thr > 0.0f) {
-                nContrib++;
-                const float eta = S.etas[b];
-                const float dadwv = dadw_out_of_line<K>(ch, xs, S.p_light, fd.p, S.events, eta);
-                const V3<float> vl = vertex<float, K>(ch, xs, K - 1);
-                const float cosv = fmaxf(vdot(vnormalize(vl - p), v3f<float>(fd.ng)), 0.0f);
-                float contrib = thr * S.lightIntensity / dadwv * cosv;
-                contrib = fminf(contrib, S.radianceClamp);
-                atomicAdd(S.spectral + (size_t)r.pixel * B + b, contrib);
             }
         }
     }
-    if (a.s.stats) {
-        flush_count(a.s.stats + 1, nConv);
-        flush_count(a.s.stats + 2, nContrib);
-    }
+    if (a.s.stats) flush_count(a.s.stats + 1, nConv);
     if (a.counters) {
         flush_count(a.counters + kCntNewton2, cNewton);
         flush_count(a.counters + kCntPolish, cPolish);
+    }
+}
+
+template <int K, bool kMulti>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_p2_vis(BatchArgs a)
+{
+    __shared__ uint32_t cand[kWarpsPerBlock][kMaxCand];
+    __shared__ uint32_t front[kWarpsPerBlock][2 * kFront];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned long long nB = min(a.p2[1], a.blockCapacity);
+    const auto* recs = reinterpret_cast<const PairRec<K>*>(a.records);
+    auto* acc = reinterpret_cast<Accepted<K>*>(a.accepted);
+    const auto* blocks = reinterpret_cast<const AcceptBlock*>(a.blocks);
+    unsigned long long cQueries = 0, cOverflow = 0, cCand = 0;
+    for (;;) {
+        unsigned long long bi = 0;
+        if (lane == 0) bi = atomicAdd(a.p2 + 3, 1ull);
+        bi = __shfl_sync(0xFFFFFFFFu, bi, 0);
+        if (bi >= nB) break;
+        const AcceptBlock blk = blocks[bi];
+        const PairRec<K>& r = recs[blk.rec];
+        const SolveArgs& S = kMulti ? a.scenes[r.scene].s : a.s;
+        const uint32_t root = __ldg(S.root);
+        const int4 ti = S.cache.tris[r.slot];
+        const int tix[4] = {ti.x, ti.y, ti.z, ti.w};
+        Chain<K> ch;
+        load_chain<K>(ch, S.tris, S.attribs, tix);
+        const float3 pe = S.fds[r.pixel].p;
+        const bool mine = (uint32_t)lane < blk.count;
+        float thr = 0.0f;
+        float xs[2 * K];
+        if (mine) {
+            const Accepted<K>& e = acc[blk.first + lane];
+            thr = e.thr;
+#pragma unroll
+            for (int i = 0; i < 2 * K; i++) xs[i] = e.x[i];
+        }
+        // one fattened query per path segment, shared by the block's roots; the segment
+        // endpoints are the chain's vertices and shading normals (contributableThroughput,
+        // pk.h:763-789)
+        for (int s = 0; s < K + 1; s++) {
+            const uint32_t valid = __ballot_sync(0xFFFFFFFFu, thr > 0.0f);
+            if (!valid) break;
+            const int leader = __ffs(valid) - 1;
+            float3 sa = mk3(0.f, 0.f, 0.f), sb = mk3(0.f, 0.f, 0.f);
+            if (thr > 0.0f) {
+                float3 va, na, vb, nb;
+                chain_vertex<K>(ch, xs, S.p_light, pe, s, va, na);
+                chain_vertex<K>(ch, xs, S.p_light, pe, s + 1, vb, nb);
+                shadow_segment(va, na, vb, nb, sa, sb);
+            }
+            const float3 ra = mk3(__shfl_sync(0xFFFFFFFFu, sa.x, leader), __shfl_sync(0xFFFFFFFFu, sa.y, leader),
+                                  __shfl_sync(0xFFFFFFFFu, sa.z, leader));
+            const float3 rb = mk3(__shfl_sync(0xFFFFFFFFu, sb.x, leader), __shfl_sync(0xFFFFFFFFu, sb.y, leader),
+                                  __shfl_sync(0xFFFFFFFFu, sb.z, leader));
+            float rad = 0.0f, mag = 0.0f;
+            if (thr > 0.0f) {
+                const float3 da = vabs(sa - ra), db = vabs(sb - rb);
+                rad = fmaxf(fmaxf(fmaxf(da.x, da.y), da.z), fmaxf(fmaxf(db.x, db.y), db.z));
+                const float3 ma = vabs(sa), mb = vabs(sb);
+                mag = fmaxf(fmaxf(fmaxf(ma.x, ma.y), ma.z), fmaxf(fmaxf(mb.x, mb.y), mb.z));
+            }
+            rad = warp_max(rad);
+            mag = warp_max(mag);
+            rad += 1.0e-5f * (1.0f + mag);  // covers the rounding of the slab and box arithmetic
+            const int nc = fat_query(S.nodes, root, ra, rb, rad, cand[warp], front[warp]);
+            __syncwarp();
+            if (lane == 0) {
+                cQueries++;
+                if (nc < 0) cOverflow++;
+                else cCand += (unsigned long long)nc;
+            }
+            if (thr > 0.0f) {
+                const float3 d = ex::sub3(sb, sa);
+                bool occ = false;
+                if (nc < 0) {
+                    occ = any_hit(S.nodes, S.tris, root, sa, d, 1.0f) < 1.0f;
+                } else {
+                    for (int c = 0; c < nc && !occ; c++) {
+                        float3 v0, v1, v2;
+                        load_tri(S.tris, cand[warp][c], v0, v1, v2);
+                        float t, u, v;
+                        float3 ng;
+                        if (ray_triangle(&t, &u, &v, &ng, 0.0f, 1.0f, sa, d, v0, v1, v2) && t < 1.0f) occ = true;
+                    }
+                }
+                if (occ) thr = 0.0f;
+            }
+            __syncwarp();
+        }
+        if (mine && !(thr > 0.0f)) acc[blk.first + lane].thr = 0.0f;
+    }
+    if (a.counters) {
         flush_count(a.counters + kCntQueries, cQueries);
         flush_count(a.counters + kCntFatOverflow, cOverflow);
         flush_count(a.counters + kCntCandidates, cCand);
     }
 }
 
+template <int K, bool kMulti>
+__global__ void __launch_bounds__(256) k_p2_contrib(BatchArgs a)
+{
+    const int B = a.s.nBins;
+    const unsigned long long n = min(a.p2[0], a.acceptCapacity);
+    const auto* recs = reinterpret_cast<const PairRec<K>*>(a.records);
+    const auto* acc = reinterpret_cast<const Accepted<K>*>(a.accepted);
+    unsigned long long nContrib = 0;
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const Accepted<K> e = acc[i];
+        if (!(e.thr > 0.0f)) continue;
+        const PairRec<K>& r = recs[e.rec];
+        const SolveArgs& S = kMulti ? a.scenes[r.scene].s : a.s;
+        const int4 ti = S.cache.tris[r.slot];
+        const int tix[4] = {ti.x, ti.y, ti.z, ti.w};
+        Chain<K> ch;
+        load_chain<K>(ch, S.tris, S.attribs, tix);
+        const FirstDiffuse fd = S.fds[r.pixel];
+        const V3<float> p = v3f<float>(fd.p);
+        const float eta = S.etas[e.bin];
+        const float dadwv = dadw_out_of_line<K>(ch, e.x, S.p_light, fd.p, S.events, eta);
+        const V3<float> vl = vertex<float, K>(ch, e.x, K - 1);
+        const float cosv = fmaxf(vdot(vnormalize(vl - p), v3f<float>(fd.ng)), 0.0f);
+        float contrib = e.thr * S.lightIntensity / dadwv * cosv;
+        contrib = fminf(contrib, S.radianceClamp);
+        atomicAdd(S.spectral + (size_t)r.pixel * B + e.bin, contrib);
+        nContrib++;
+    }
+    if (a.s.stats) flush_count(a.s.stats + 2, nContrib);
+}
+
+template <int K, bool kMulti>
+static cudaError_t launch_phases(const BatchArgs& a, int blocksPerSM, int p1BlocksPerSM, cudaStream_t s)
+{
+    const int sms = num_sms();
+    k_probe<K, kMulti><<<sms * 2 * p1BlocksPerSM, 256, 0, s>>>(a);
+    k_phase1<K, kMulti><<<sms * p1BlocksPerSM, 256, 0, s>>>(a);
+    for (int w = 0; w < kMaxWaves; w++) {
+        cudaError_t e = cudaMemsetAsync(a.p2, 0, 4 * sizeof(unsigned long long), s);
+        if (e != cudaSuccess) return e;
+        k_p2_solve<K, kMulti><<<sms * blocksPerSM, kWarpsPerBlock * 32, 0, s>>>(a);
+        k_p2_vis<K, kMulti><<<sms * 4, kWarpsPerBlock * 32, 0, s>>>(a);
+        k_p2_contrib<K, kMulti><<<sms * 8, 256, 0, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
 template <int K>
 static cudaError_t launch_k(const BatchArgs& a, int blocksPerSM, cudaStream_t s, int p1BlocksPerSM = 8)
 {
-    if (a.scenes) {
-        k_probe<K, true><<<num_sms() * 2 * p1BlocksPerSM, 256, 0, s>>>(a);
-        k_phase1<K, true><<<num_sms() * p1BlocksPerSM, 256, 0, s>>>(a);
-        k_phase2<K, true><<<num_sms() * blocksPerSM, kWarpsPerBlock * 32, 0, s>>>(a);
-    } else {
-        k_probe<K, false><<<num_sms() * 2 * p1BlocksPerSM, 256, 0, s>>>(a);
-        k_phase1<K, false><<<num_sms() * p1BlocksPerSM, 256, 0, s>>>(a);
-        k_phase2<K, false><<<num_sms() * blocksPerSM, kWarpsPerBlock * 32, 0, s>>>(a);
-    }
-    return cudaGetLastError();
+    if (a.scenes) return launch_phases<K, true>(a, blocksPerSM, p1BlocksPerSM, s);
+    return launch_phases<K, false>(a, blocksPerSM, p1BlocksPerSM, s);
 }
 
 size_t probe_bytes(int K)
@@ -786,6 +913,19 @@ size_t probe_bytes(int K)
         default: return 0;
     }
 }
+
+size_t accepted_bytes(int K)
+{
+    switch (K) {
+        case 1: return sizeof(Accepted<1>);
+        case 2: return sizeof(Accepted<2>);
+        case 3: return sizeof(Accepted<3>);
+        case 4: return sizeof(Accepted<4>);
+        default: return 0;
+    }
+}
+
+size_t block_bytes() { return sizeof(AcceptBlock); }
 
 size_t record_bytes(int K)
 {

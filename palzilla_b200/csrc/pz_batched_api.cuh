@@ -25,7 +25,26 @@ struct BatchArgs {
     const SceneArgs* scenes = nullptr; // batch of scenes (device table), or null: the single scene s
     uint32_t nScenes = 0;
     const unsigned long long* offsets = nullptr;  // nScenes + 1 item offsets of the batch
+    // phase 2: accepted roots and their per-round blocks, reused by every wave
+    void* accepted = nullptr;          // acceptCapacity entries of accepted_bytes(K)
+    unsigned long long acceptCapacity = 0;
+    void* blocks = nullptr;            // blockCapacity entries of block_bytes()
+    unsigned long long blockCapacity = 0;
+    unsigned long long* p2 = nullptr;  // device u64[4]: accepted count, block count, reserved, blocks taken
 };
+
+// Phase 2 runs in at most kMaxWaves waves; each wave has room for 64 accepted roots (a record's
+// most) per record of 1/kMaxWaves of the record capacity, so every record fits.
+constexpr int kMaxWaves = 8;
+inline unsigned long long accept_capacity(unsigned long long recordCapacity)
+{
+    return 64ull * ((recordCapacity + kMaxWaves - 1) / kMaxWaves);
+}
+// at most two rounds (blocks) per record: B <= 64 bins, 32 lanes
+inline unsigned long long block_capacity(unsigned long long recordCapacity)
+{
+    return 2ull * ((recordCapacity + kMaxWaves - 1) / kMaxWaves);
+}
 
 // One scene of a batch: its solve arguments and its item count on the device.
 struct SceneArgs {
@@ -41,6 +60,9 @@ enum {
 
 // bytes of one phase-1 record for chain length K
 size_t record_bytes(int K);
+// bytes of one accepted phase-2 root, and of one block of them
+size_t accepted_bytes(int K);
+size_t block_bytes();
 // bytes of one plain-solve probe (root and verdict) for chain length K
 size_t probe_bytes(int K);
 cudaError_t launch_solve_batched(int K, const BatchArgs& a, int blocksPerSM, cudaStream_t s);

@@ -223,11 +223,30 @@ extern "C" int pz_solve_specular_plain(const pz_solve_desc* desc, pz_stream_t st
     return done(launch(desc->K, desc->spectral != nullptr, a, S(stream)), "pz_solve_specular_plain");
 }
 
+namespace {
+// Scratch of one batched solve: 256-byte header | phase-1 records (one per work item) |
+// plain-solve probes (three per work item) | phase-2 accepted roots | their blocks, each
+// region 256-byte aligned.
+struct BatchLayout {
+    size_t records, probes, accepted, blocks, total;
+};
+inline size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
+BatchLayout batch_layout(int K, uint64_t maxPaths, size_t start)
+{
+    BatchLayout L;
+    L.records = start;
+    L.probes = L.records + a256((size_t)maxPaths * batched::record_bytes(K));
+    L.accepted = L.probes + a256((size_t)maxPaths * 3 * batched::probe_bytes(K));
+    L.blocks = L.accepted + a256((size_t)batched::accept_capacity(maxPaths) * batched::accepted_bytes(K));
+    L.total = L.blocks + a256((size_t)batched::block_capacity(maxPaths) * batched::block_bytes());
+    return L;
+}
+}  // namespace
+
 extern "C" size_t pz_solve_batched_scratch_bytes(int K, uint64_t max_paths)
 {
     if (K < 1 || K > 4) return 0;
-    // header | one phase-1 record per work item | three plain-solve probes per work item
-    return 256 + (size_t)max_paths * (batched::record_bytes(K) + 3 * batched::probe_bytes(K));
+    return batch_layout(K, max_paths, 256).total;
 }
 
 extern "C" int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32_t* n_paths_dev, void* scratch_dev,
@@ -248,9 +267,15 @@ extern "C" int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32
     b.status = reinterpret_cast<uint32_t*>(base);
     b.workCounter = reinterpret_cast<unsigned long long*>(base + 8);
     b.recordCount = reinterpret_cast<unsigned long long*>(base + 16);
-    b.records = base + 256;
+    const BatchLayout L = batch_layout(desc->K, desc->n_paths, 256);
+    b.records = base + L.records;
     b.recordCapacity = desc->n_paths;
-    b.probes = base + 256 + (size_t)desc->n_paths * batched::record_bytes(desc->K);
+    b.probes = base + L.probes;
+    b.accepted = base + L.accepted;
+    b.acceptCapacity = batched::accept_capacity(desc->n_paths);
+    b.blocks = base + L.blocks;
+    b.blockCapacity = batched::block_capacity(desc->n_paths);
+    b.p2 = reinterpret_cast<unsigned long long*>(base + 160);
     b.nPathsDev = n_paths_dev;
     static_assert(64 + 8 * batched::kNumCounters <= 256, "counters live in the 256-byte scratch header");
     b.counters = reinterpret_cast<unsigned long long*>(base + 64);
@@ -289,16 +314,19 @@ namespace {
 constexpr size_t kMultiHeader = 256;
 inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 struct MultiLayout {
-    size_t offsets, table, records, probes, total;
+    size_t offsets, table, records, probes, accepted, blocks, total;
 };
 MultiLayout multi_layout(int K, uint32_t nScenes, uint64_t maxPaths)
 {
     MultiLayout L;
     L.offsets = kMultiHeader;
     L.table = L.offsets + align256(8 * ((size_t)nScenes + 1));
-    L.records = L.table + align256(sizeof(batched::SceneArgs) * (size_t)nScenes);
-    L.probes = L.records + align256((size_t)maxPaths * batched::record_bytes(K));
-    L.total = L.probes + align256((size_t)maxPaths * 3 * batched::probe_bytes(K));
+    const BatchLayout B = batch_layout(K, maxPaths, L.table + align256(sizeof(batched::SceneArgs) * (size_t)nScenes));
+    L.records = B.records;
+    L.probes = B.probes;
+    L.accepted = B.accepted;
+    L.blocks = B.blocks;
+    L.total = B.total;
     return L;
 }
 
@@ -369,6 +397,11 @@ static int multi_args(int K, int n_bins, uint32_t n_scenes, uint64_t total, void
     b->records = base + L.records;
     b->recordCapacity = total;
     b->probes = base + L.probes;
+    b->accepted = base + L.accepted;
+    b->acceptCapacity = batched::accept_capacity(total);
+    b->blocks = base + L.blocks;
+    b->blockCapacity = batched::block_capacity(total);
+    b->p2 = reinterpret_cast<unsigned long long*>(base + 160);
     b->polishDet = 0.0;
     b->grazeCos = 0.0f;
     b->continuation = 0;
@@ -430,7 +463,7 @@ extern "C" int pz_solve_multi_autotune(int K, int n_bins, uint32_t n_scenes, uin
     pz_batch_tuning best = {8, 2, 1};
     float bestMs = 3.4e38f;
     cudaError_t e = run_multi(K, b, best, offsets, scratch_dev, s);  // warm-up
-    const int p1s[] = {4, 8, 16}, p2s[] = {1, 2}, chunks[] = {1, 4};
+    const int p1s[] = {4, 8, 16}, p2s[] = {1, 2}, chunks[] = {1};
     for (int p1 : p1s)
         for (int p2 : p2s)
             for (int c : chunks) {

@@ -28,7 +28,7 @@ __global__ void __launch_bounds__(256) k_solve_constraints(uint32_t events, floa
                                                            const float* __restrict__ etas, uint32_t n,
                                                            const pz_triangle* __restrict__ tris,
                                                            const pz_triangle_attrib* __restrict__ attribs,
-                                                           int maxIterations, float costTolerance, int warmup,
+                                                           uint32_t nTris, int maxIterations, float costTolerance, int warmup,
                                                            float* __restrict__ params, uint8_t* __restrict__ converged,
                                                            int32_t* __restrict__ iters)
 {
@@ -36,6 +36,14 @@ __global__ void __launch_bounds__(256) k_solve_constraints(uint32_t events, floa
     if (i >= n) return;
     pz_triangle tk[K];
     pz_triangle_attrib ak[K];
+    bool valid = true;
+#pragma unroll
+    for (int k = 0; k < K; k++) valid = valid && (uint32_t)tuples[(size_t)i * K + k] < nTris;
+    if (!valid) {  // a triangle index out of range: the item is not solved
+        if (converged) converged[i] = 0;
+        if (iters) iters[i] = -2;
+        return;
+    }
 #pragma unroll
     for (int k = 0; k < K; k++) {
         const int32_t t = tuples[(size_t)i * K + k];
@@ -57,10 +65,11 @@ __global__ void __launch_bounds__(256) k_solve_constraints(uint32_t events, floa
 
 template <int K>
 cudaError_t launch(uint32_t events, float3 p_beg, const int32_t* tuples, const float3* p_end, const float* etas,
-                   uint32_t n, const pz_triangle* tris, const pz_triangle_attrib* attribs, int maxIterations,
-                   float tol, int warmup, float* params, uint8_t* conv, int32_t* iters, cudaStream_t s)
+                   uint32_t n, const pz_triangle* tris, const pz_triangle_attrib* attribs, uint32_t nTris,
+                   int maxIterations, float tol, int warmup, float* params, uint8_t* conv, int32_t* iters,
+                   cudaStream_t s)
 {
-    k_solve_constraints<K><<<(n + 255) / 256, 256, 0, s>>>(events, p_beg, tuples, p_end, etas, n, tris, attribs,
+    k_solve_constraints<K><<<(n + 255) / 256, 256, 0, s>>>(events, p_beg, tuples, p_end, etas, n, tris, attribs, nTris,
                                                            maxIterations, tol, warmup, params, conv, iters);
     return cudaGetLastError();
 }
@@ -73,7 +82,7 @@ using namespace pz;
 extern "C" int pz_solve_constraints(int K, uint32_t events, pz_float3 p_beg, const int32_t* tuples_dev,
                                     const pz_float3* p_end_dev, const float* etas_dev, uint32_t n,
                                     const pz_triangle* triangles_dev, const pz_triangle_attrib* attribs_dev,
-                                    int max_iterations, float cost_tolerance, int early_term_warmup, float* params_dev,
+                                    uint32_t n_triangles, int max_iterations, float cost_tolerance, int early_term_warmup, float* params_dev,
                                     uint8_t* converged_dev, int32_t* iters_dev, pz_stream_t stream)
 {
     if (K < 1 || K > 4) return fail(PZ_ERR_INVALID_ARGUMENT, "pz_solve_constraints: K must be 1..4 (got %d)", K);
@@ -91,13 +100,13 @@ extern "C" int pz_solve_constraints(int K, uint32_t events, pz_float3 p_beg, con
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     cudaError_t e = cudaErrorInvalidValue;
     switch (K) {
-        case 1: e = launch<1>(events, pb, tuples_dev, pe, etas_dev, n, triangles_dev, attribs_dev, max_iterations,
+        case 1: e = launch<1>(events, pb, tuples_dev, pe, etas_dev, n, triangles_dev, attribs_dev, n_triangles, max_iterations,
                               cost_tolerance, early_term_warmup, params_dev, converged_dev, iters_dev, s); break;
-        case 2: e = launch<2>(events, pb, tuples_dev, pe, etas_dev, n, triangles_dev, attribs_dev, max_iterations,
+        case 2: e = launch<2>(events, pb, tuples_dev, pe, etas_dev, n, triangles_dev, attribs_dev, n_triangles, max_iterations,
                               cost_tolerance, early_term_warmup, params_dev, converged_dev, iters_dev, s); break;
-        case 3: e = launch<3>(events, pb, tuples_dev, pe, etas_dev, n, triangles_dev, attribs_dev, max_iterations,
+        case 3: e = launch<3>(events, pb, tuples_dev, pe, etas_dev, n, triangles_dev, attribs_dev, n_triangles, max_iterations,
                               cost_tolerance, early_term_warmup, params_dev, converged_dev, iters_dev, s); break;
-        case 4: e = launch<4>(events, pb, tuples_dev, pe, etas_dev, n, triangles_dev, attribs_dev, max_iterations,
+        case 4: e = launch<4>(events, pb, tuples_dev, pe, etas_dev, n, triangles_dev, attribs_dev, n_triangles, max_iterations,
                               cost_tolerance, early_term_warmup, params_dev, converged_dev, iters_dev, s); break;
     }
     return done(e, "pz_solve_constraints");

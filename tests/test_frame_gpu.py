@@ -71,8 +71,9 @@ def test_trace_closest_and_any(orc, which):
     assert np.array_equal(_np(ng, np.float32), exp["ng"])
     tmax = np.random.default_rng(2).uniform(0.5, 4.0, n).astype(np.float32)
     hit = torch.empty(n, dtype=torch.uint8, device="cuda")
+    dtmax = torch.from_numpy(tmax).cuda()  # held until the kernel has run
     A._lib.call("pz_trace_any", A._vp(ds.internals), A._vp(ds.root_dev), A._vp(ds.tris), n, A._vp(dro),
-                A._vp(drd), A._vp(torch.from_numpy(tmax).cuda()), A._vp(hit), None)
+                A._vp(drd), A._vp(dtmax), A._vp(hit), None)
     torch.cuda.synchronize()
     assert np.array_equal(hit.cpu().numpy(), orc.trace_any(bvh["nodes"], bvh["root"], sc.tris, ro, rd, tmax))
 

@@ -49,8 +49,9 @@ def test_rays_and_photons_match_golden(g):
     A._lib.call("pz_trace_closest", A._vp(ds.internals), A._vp(ds.root_dev), A._vp(ds.tris), n, A._vp(ro),
                 A._vp(rd), A._vp(t), A._vp(uv), A._vp(tri), A._vp(ng), A._vp(status), None)
     hit = torch.empty(n, dtype=torch.uint8, device="cuda")
+    tmax = torch.from_numpy(g["ray_tmax"]).cuda()  # held until the kernel has run
     A._lib.call("pz_trace_any", A._vp(ds.internals), A._vp(ds.root_dev), A._vp(ds.tris), n, A._vp(ro), A._vp(rd),
-                A._vp(torch.from_numpy(g["ray_tmax"]).cuda()), A._vp(hit), None)
+                A._vp(tmax), A._vp(hit), None)
     torch.cuda.synchronize()
     assert int(status.item()) == 0
     assert t.cpu().numpy().tobytes() == g["hit_t"].tobytes()

@@ -62,7 +62,8 @@ def test_pack_against_oracle(orc):
     acc[:, 3] = rng.integers(1, 65, n).astype(np.float32)
     acc[: n // 8, :3] *= 1e-3  # the linear segment of the OETF
     pixels = torch.zeros(n, dtype=torch.int32, device="cuda")
-    _lib.call("pz_resolve", A._vp(pixels), A._vp(torch.from_numpy(acc).cuda()), n, None)
+    acc_d = torch.from_numpy(acc).cuda()  # held until the kernel has run
+    _lib.call("pz_resolve", A._vp(pixels), A._vp(acc_d), n, None)
     torch.cuda.synchronize()
     got = pixels.cpu().numpy().view(np.uint32)
     exp = orc.pack(acc)
@@ -79,7 +80,8 @@ def test_resolve_spectral_against_oracle(orc):
     rgb = torch.zeros((n, 4), device="cuda")
     pixels = torch.zeros(n, dtype=torch.int32, device="cuda")
     albedo = (0.75, 0.7, 0.65)
-    _lib.call("pz_resolve_spectral", A._vp(rgb), A._vp(pixels), A._vp(torch.from_numpy(spectral).cuda()), n, nb,
+    spectral_d = torch.from_numpy(spectral).cuda()  # held until the kernel has run
+    _lib.call("pz_resolve_spectral", A._vp(rgb), A._vp(pixels), A._vp(spectral_d), n, nb,
               _lib.f32(380.0), _lib.f32(780.0), _lib.f3(albedo), None)
     torch.cuda.synchronize()
     rgb_o, px_o = orc.resolve_spectral(spectral, 380.0, 780.0, albedo)

@@ -8,10 +8,11 @@ oracle from the same initial barycentrics; the FP64 error stated beside it).
   fresh two-refraction tuples;
 * the roots of every (item, bin) the plain solve converged on (pz_solve_desc.roots) against
   the oracle's solve from the photon's barycentrics, bit for bit;
-* the batched solve's solved vertices (refined from predictions for bins deep inside the
-  triangles, solved from the photon's barycentrics otherwise) within 1e-5 relative of the
-  plain solve's wherever both converged, and a root for every (item, bin) that contributes
-  to the plain image.
+* the batched solve's roots: bins solved from the photon's barycentrics bit for bit equal to
+  the plain roots; bins refined from a predicted root (deep inside the triangles) start
+  elsewhere and stop at another point within the cost tolerance, so their solved vertices are
+  held within 1e-5 relative of the FP64 root; and a root for every (item, bin) that
+  contributes to the plain image.
 """
 import os
 
@@ -30,17 +31,23 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "gol
 
 
 def _solve_device(K, ev, p_beg, tuples, params, p_end, etas, tris, attribs, max_iter=32, tol=1e-10, warmup=1):
+    """pz_solve_constraints over a batch; every device buffer is held in a local until the
+    kernel has finished (a pointer taken from a temporary tensor would be freed, and its
+    memory handed to the next allocation, before the launch)."""
     n = len(tuples)
     t_tris = torch.from_numpy(np.ascontiguousarray(tris, np.float32)).cuda()
     t_att = torch.from_numpy(np.ascontiguousarray(attribs).view(np.uint8).reshape(-1)).cuda()
+    t_tup = torch.from_numpy(np.ascontiguousarray(tuples, np.int32).reshape(n, K)).cuda()
+    t_end = torch.from_numpy(np.ascontiguousarray(p_end, np.float32).reshape(n, 3)).cuda()
+    t_eta = torch.from_numpy(np.ascontiguousarray(etas, np.float32).reshape(n)).cuda()
     prm = torch.from_numpy(np.ascontiguousarray(params, np.float32).reshape(n, 2 * K)).cuda()
     conv = torch.zeros(n, dtype=torch.uint8, device="cuda")
     its = torch.zeros(n, dtype=torch.int32, device="cuda")
-    _lib.call("pz_solve_constraints", K, ev, _lib.f3(p_beg),
-              A._vp(torch.from_numpy(np.ascontiguousarray(tuples, np.int32)).cuda()),
-              A._vp(torch.from_numpy(np.ascontiguousarray(p_end, np.float32)).cuda()),
-              A._vp(torch.from_numpy(np.ascontiguousarray(etas, np.float32)).cuda()), n, A._vp(t_tris), A._vp(t_att),
-              max_iter, _lib.f32(tol), warmup, A._vp(prm), A._vp(conv), A._vp(its), None)
+    n_tris = int(t_tris.numel() // 9)
+    assert t_att.numel() == 40 * n_tris and int(np.max(tuples)) < n_tris and int(np.min(tuples)) >= 0
+    _lib.call("pz_solve_constraints", K, ev, _lib.f3(p_beg), A._vp(t_tup), A._vp(t_end), A._vp(t_eta), n,
+              A._vp(t_tris), A._vp(t_att), n_tris, max_iter, _lib.f32(tol), warmup, A._vp(prm), A._vp(conv),
+              A._vp(its), None)
     torch.cuda.synchronize()
     return conv.cpu().numpy().astype(bool), prm.cpu().numpy(), its.cpu().numpy()
 
@@ -145,25 +152,41 @@ def test_plain_and_batched_roots(orc, events):
                 assert got.tobytes() == x.astype(np.float32).tobytes(), (i, b, got, x)
                 checked += 1
     assert checked > 50
-    # batched solved vertices within 1e-5 relative of the plain ones wherever both converged
+    # batched roots: a bin solved from the photon's barycentrics equals the plain root bit for
+    # bit; a bin refined from its predicted root stops at another point of the cost tolerance
+    # (cost < 1e-10), so it is held to the FP64 root (double Newton to 1e-24 from it): solved
+    # vertices within 1e-5 relative, as the plain root itself is to the same FP64 root
     p, q = roots["plain"], roots["batched"]
     both = np.isfinite(p).all(-1) & np.isfinite(q).all(-1)
     assert both.sum() > 100
-    it, bn = np.nonzero(both)
-    tup = gc["tris"][pairs[it, 1], :K]
-    dev = np.zeros(len(it))
-    for k in range(K):
-        t = sc.tris[tup[:, k]].astype(np.float64).reshape(-1, 3, 3)
+    same = both & (p == q).all(-1)
+    it, bn = np.nonzero(both & ~same)
+    sel = rng.choice(len(it), size=min(len(it), 1500), replace=False) if len(it) else np.zeros(0, int)
+    etas_h = sc.bin_etas()
 
-        def vertex(x):
-            u, v = x[:, 2 * k].astype(np.float64), x[:, 2 * k + 1].astype(np.float64)
-            return t[:, 0] + (t[:, 1] - t[:, 0]) * u[:, None] + (t[:, 2] - t[:, 0]) * v[:, None]
-        vp, vq = vertex(p[it, bn]), vertex(q[it, bn])
-        dev = np.maximum(dev, np.linalg.norm(vp - vq, axis=1) / np.linalg.norm(vp, axis=1))
-    assert float(dev.max()) <= 1e-5, float(dev.max())
+    def vertices(x, tup):
+        out = []
+        for k in range(K):
+            t = sc.tris[tup[k]].astype(np.float64).reshape(3, 3)
+            out.append(t[0] + (t[1] - t[0]) * float(x[2 * k]) + (t[2] - t[0]) * float(x[2 * k + 1]))
+        return np.array(out)
+
+    worst_b, worst_p = 0.0, 0.0
+    for s_ in sel:
+        i, b = it[s_], bn[s_]
+        px, slot = pairs[i]
+        tup = gc["tris"][slot, :K]
+        o, x64, _ = orc.solve_constraints(K, q[i, b].astype(np.float64), L, fd[px, :3], sc.tris[tup], sc.attribs[tup],
+                                          float(etas_h[b]), ev, max_iter=8, tol=1e-24, warmup=64, dtype=np.float64)
+        v64 = vertices(x64, tup)
+        scale = np.linalg.norm(v64, axis=1)
+        worst_b = max(worst_b, float((np.linalg.norm(vertices(q[i, b], tup) - v64, axis=1) / scale).max()))
+        worst_p = max(worst_p, float((np.linalg.norm(vertices(p[i, b], tup) - v64, axis=1) / scale).max()))
+    assert worst_b <= 1e-5, worst_b
     # every (item, bin) that contributes to the plain image has a batched root
     contrib = orc.render_each(K, pairs, gc, fd, orc.build_bvh(sc.tris), sc, sc.bin_etas(), dtype=np.float32) > 0
     assert contrib.any()
     assert np.isfinite(q[contrib]).all(-1).all()
-    print(f"\n[{events}] plain roots bitwise on {checked} (item, bin); batched within {float(dev.max()):.1e} "
-          f"on {int(both.sum())} roots")
+    print(f"\n[{events}] plain roots bitwise on {checked} (item, bin); batched roots: {int(same.sum())} of "
+          f"{int(both.sum())} bitwise equal to the plain ones, the others within {worst_b:.1e} (vertex, relative) of "
+          f"the FP64 root, where the plain roots are within {worst_p:.1e}")
