@@ -48,8 +48,9 @@ WORKLOAD = {
 }
 POLISH_DET = 1.0e-6
 # kernels of this library launched per frame: k_primary, k_photon, k_lookup, sort k_hist + 4 x k_pass,
-# k_reorder, k_probe, k_phase1, k_phase2, k_resolve_spectral
-LAUNCHES_PER_FRAME = 13
+# k_reorder, k_probe, k_phase1, 8 phase-2 waves x (k_p2_solve, k_p2_vis, k_p2_contrib) (waves
+# without records exit at once), k_resolve_spectral
+LAUNCHES_PER_FRAME = 12 + 8 * 3
 # DRAM bytes (read + write) per work item of k_probe + k_phase1 + k_phase2, from one ncu
 # capture of the first frame of this workload (its light sample is the centre):
 # 6971.2 MB / 19.8 M items
@@ -147,10 +148,12 @@ def reduce(world, v: float, op: str) -> float:
     return float(t.item())
 
 
-def sphere():
+def sphere(image: int = 0):
     from palzilla_b200 import scenes as S
     sc = S.sphere_scene()
     sc.photons_per_triangle = 205
+    if image:
+        sc.width = sc.height = image
     return sc
 
 
@@ -158,8 +161,9 @@ def sphere():
 class Renderer:
     """One frame of the hot path on the current device (all buffers allocated up front)."""
 
-    def __init__(self, sc):
+    def __init__(self, sc, fold_det: float = 0.0):
         import torch
+        self.fold_det = fold_det
         from palzilla_b200 import api as A
         from palzilla_b200.scenes import event_descriptor
         self.A, self.sc = A, sc
@@ -195,7 +199,7 @@ class Renderer:
         self.spectral.zero_()
         d = A.solve_desc(self.ds, self.frame, self.cache, sc.events, self.n_paths, spectral=self.spectral,
                          etas=self.etas, stats=self.stats, exact=exact, iteration=self.iteration,
-                         polish_det=0.0 if plain else POLISH_DET)
+                         polish_det=0.0 if plain else POLISH_DET, fold_det=self.fold_det)
         if solve_events:
             solve_events[0].record()
         if plain:
@@ -214,8 +218,8 @@ class Renderer:
 def run_ours(args):
     import torch
     world, rank, local = setup_dist()
-    sc = sphere()
-    R = Renderer(sc)
+    sc = sphere(args.image)
+    R = Renderer(sc, fold_det=args.fold_det)
 
     def ev():
         return torch.cuda.Event(enable_timing=True)
@@ -255,6 +259,12 @@ def run_ours(args):
     p_ms, p_paths, p_solve_ms = timed_frames(kp, 100, plain=True)
     p_tmax = reduce(world, p_ms, "max")
     p_value = reduce(world, p_paths, "sum") / (p_tmax / 1e3)
+
+    # ---- the reference's own plain per-tuple solve kernel (solveSpecularPath_K2 of main_gpu.cu,
+    # compiled for sm_100a with the compiler's default contraction, as its run-time compile
+    # builds it) on the same work list: one launch per bin, each with the pixels' wavelength set
+    # to the bin's centre, so eta = cauchy(lambda_b) is the bin's eta.  Solve stage only.
+    ref_gpu = reference_gpu_solve(R, steps=kp) if rank == 0 and world == 1 and not args.no_ref_gpu else None
 
     # ---- image agreement on identical solver inputs (one PathCache and work list).  The photon
     # pass itself is not deterministic: the first photon to claim a PathCache slot supplies the
@@ -319,7 +329,9 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": dict(WORKLOAD, parallelism=f"{world} independent frame replicas" if world > 1 else "1 GPU"),
+            "config": dict(WORKLOAD, image=f"{sc.width}x{sc.height}",
+                           parallelism=f"{world} independent frame replicas" if world > 1 else "1 GPU",
+                           **({"fold_det": args.fold_det} if args.fold_det else {})),
             "ms_per_frame": t_max / args.steps,
             "work_items_per_frame": n_items,
             "path_solves_per_frame": paths / args.steps,
@@ -328,6 +340,12 @@ def run_ours(args):
                       "steps": kp},
             "speedup_paths_per_s_vs_plain": value / p_value,
             "speedup_solve_vs_plain": float(np.mean(p_solve_ms)) / solve_avg,
+            "reference_gpu_plain": None if ref_gpu is None else dict(
+                ref_gpu, speedup_solve=ref_gpu["solve_ms_per_frame"] / solve_avg,
+                speedup_paths_per_s=(t_max / args.steps - solve_avg + ref_gpu["solve_ms_per_frame"]) /
+                (t_max / args.steps),
+                frame_note="frame-level speed-up: this frame with its solve stage replaced by the reference "
+                           "kernel's"),
             "image_rel_rmse": rmse,
             "batched_counters": counters,
             "e2e": {"value": e2e_paths / (e2e_ms / 1e3), "unit": UNIT, "steps": ke, "ms_per_step": e2e_ms / ke,
@@ -344,6 +362,43 @@ def run_ours(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def reference_gpu_solve(R, steps=2):
+    """Times the reference's solveSpecularPath_K<K> (default build) over the prepared frame's
+    work list for every bin: per bin, a FirstDiffuse copy with lambda set to the bin's centre."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_gpu as G
+    import torch
+    if not G.available("default"):
+        return {"unavailable": "reference GPU kernels not built (oracle/build_ref_gpu.sh needs the reference sources)"}
+    rg = G.RefGpu("default")
+    sc, fr = R.sc, R.frame
+    K = len(sc.events)
+    rc = rg.cache_from_ours(R.cache.views())
+    fds = []
+    for lam in sc.bin_lambdas():
+        f = fr.fd.clone()
+        f.view(torch.float32).view(fr.npx, 10)[:, 9] = float(lam)
+        fds.append(f)
+    accum = torch.zeros((fr.npx, 4), device="cuda")
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in fds]
+
+    def run():
+        for f, (e0, e1) in zip(fds, ev):
+            e0.record()
+            rg.solve_specular(K, accum, fr.paths, R.n_paths, f, R.ds.root_dev, R.ds.internals, R.ds.tris,
+                              R.ds.attribs, sc.light_point(R.iteration), sc.light_intensity, sc.radiance_clamp, rc,
+                              sc.cell_step, R.ev, sc.cauchy_a, sc.cauchy_b, R.iteration)
+            e1.record()
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in ev)
+    run()
+    ms = float(np.mean([run() for _ in range(max(1, steps))]))
+    del fds, rc
+    return {"solve_ms_per_frame": ms, "value": R.n_paths * sc.n_bins / (ms / 1e3), "unit": UNIT,
+            "kernel": f"solveSpecularPath_K{K} (main_gpu.cu:418-497), {sc.n_bins} launches per frame",
+            "build": "reference sources, nvcc -gencode arch=compute_100a,code=sm_100a -O3 (default FMA contraction)"}
 
 
 def bench_sort_build(hbm, hbm_kind, n=1 << 24):
@@ -817,6 +872,9 @@ def main():
     ap.add_argument("--ref-items", type=int, default=20000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-sort", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference's own GPU solve kernel")
+    ap.add_argument("--fold-det", type=float, default=0.0, help="batched solve: fold threshold (0 = the default)")
+    ap.add_argument("--image", type=int, default=0, help="image side for small profiling runs (0 = 1024)")
     ap.add_argument("--workload", default="sphere", choices=["sphere", "sort_build", "uneven_batch", "pathcuts",
                                                              "adjoint", "subdivision"],
                     help="sphere: the frame benchmark; sort_build: onesweep sort + LBVH build alone; "

@@ -55,10 +55,13 @@ def ref_dir() -> str:
 
 
 def build_ref() -> bool:
-    """Compile the reference's CPU code when its sources are present; True if the library exists."""
+    """Compile the reference's CPU code (and its GPU kernels, oracle/ref_gpu.py) when its
+    sources are present; True if the CPU library exists."""
     script = os.path.join(HERE, "build_ref.sh")
     if os.path.isdir(ref_dir()):
         subprocess.run([script], check=True, stdout=subprocess.DEVNULL, env=dict(os.environ, REF_DIR=ref_dir()))
+        import ref_gpu
+        ref_gpu.build()
     return os.path.exists(REF_SO)
 
 

@@ -45,8 +45,8 @@ namespace batched {
 #endif
 
 constexpr int kWarpsPerBlock = 8;
-constexpr int kMaxCand = 32;
-constexpr int kFront = 64;     // frontier entries per level of the breadth-first query
+constexpr int kMaxCand = 96;   // candidate (triangle, segment) entries of one merged query
+constexpr int kFront = 128;    // frontier entries per level of the breadth-first query
 constexpr float kMaxShift = 0.5f;    // a larger predicted shift over the band falls back
 constexpr float kDeep = 0.3f;        // a predicted root this far inside every triangle is refined, not re-solved
 constexpr float kProbeTol = 1.0e-3f;  // a plain-solve root farther than this from the followed branch is another root
@@ -175,44 +175,84 @@ PZ_D void shadow_segment(float3 from, float3 from_n, float3 to, float3 to_n, flo
     b = ex::add3(to, ex::mul3(to_n, ray_offset_scale(to)));
 }
 
-// Warp-cooperative query: the leaves whose box, grown by r, meets segment [a, b], found
-// breadth first.  The lanes test up to 32 nodes of the frontier at once, one tree level
-// per step, so the chain of dependent node loads is the tree's depth and not the number
-// of nodes visited (with a depth-first walk run by the whole warp, the shadow tests of
-// the dispersive-sphere frame took 1.3x as long: 114 ms against 85 ms).  Leaves and internal children that pass are appended in ballot
-// order to the candidate list and to the next level's frontier (two halves of `front`,
-// kFront entries each).  A leaf is a candidate when its box, and every ancestor's, meets
-// the fattened segment.  Returns the count, or -1 when the candidate list or the frontier
-// overflows.
-PZ_D int fat_query(const Node* __restrict__ nodes, uint32_t root, float3 a, float3 b, float r, uint32_t* cand,
-                       uint32_t* front)
+// Warp-cooperative query of NS segments at once: for each segment s, the leaves whose box,
+// grown by r[s], meets the segment [a[s], a[s] + d[s]], found breadth first.  Frontier
+// entries are (node, segment) pairs, so the lanes test the frontier nodes of every segment
+// side by side, one tree level per step: the chain of dependent node loads is the tree's
+// depth, and the frontier of one level holds the nodes of all segments (a frontier of a single
+// fattened segment is a few nodes wide, and left most lanes idle).  Leaves that pass are
+// appended to the candidate list as (triangle, segment) entries in ballot order, internal
+// children to the next level's frontier (two halves of `front`, kFront entries each); a leaf
+// is a candidate when its box, and every ancestor's, meets the fattened segment.  Entries
+// carry the segment in bits 29-31 (node and triangle indices below 2^29).  Returns the count,
+// or -1 when the candidate list or the frontier overflows.
+constexpr uint32_t kSegShift = 29;
+constexpr uint32_t kIdxMask = (1u << kSegShift) - 1u;
+
+template <int NS>
+PZ_D float3 pick3(const float3 (&v)[NS], uint32_t i)
+{
+    float3 r = v[0];
+#pragma unroll
+    for (int j = 1; j < NS; j++)
+        if (i == (uint32_t)j) r = v[j];
+    return r;
+}
+template <int NS>
+PZ_D float pick1(const float (&v)[NS], uint32_t i)
+{
+    float r = v[0];
+#pragma unroll
+    for (int j = 1; j < NS; j++)
+        if (i == (uint32_t)j) r = v[j];
+    return r;
+}
+
+template <int NS>
+PZ_D int fat_query_multi(const Node* __restrict__ nodes, uint32_t root, const float3 (&a)[NS], const float3 (&inv)[NS],
+                         const float (&r)[NS], uint32_t segMask, uint32_t* cand, uint32_t* front)
 {
     const int lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
-    if (root == kInvalidNode) return 0;
+    if (root == kInvalidNode || !segMask) return 0;
     if (is_leaf(root)) {
-        if (lane == 0) cand[0] = node_idx(root);
-        return 1;
+        int n = 0;
+#pragma unroll
+        for (int s = 0; s < NS; s++)
+            if ((segMask >> s) & 1u) {
+                if (lane == 0) cand[n] = node_idx(root) | ((uint32_t)s << kSegShift);
+                n++;
+            }
+        return n;
     }
-    const float3 d = b - a;
-    const float3 inv = inv_rd(d);
-    const float3 R = mk3(r, r, r);
-    if (lane == 0) front[0] = root;
+    int nf = 0;
+#pragma unroll
+    for (int s = 0; s < NS; s++)
+        if ((segMask >> s) & 1u) {
+            if (lane == 0) front[nf] = node_idx(root) | ((uint32_t)s << kSegShift);
+            nf++;
+        }
     __syncwarp();
-    int n = 0, nf = 1, cur = 0;
+    int n = 0, cur = 0;
     while (nf > 0) {
         int nNext = 0;
         for (int base = 0; base < nf; base += 32) {
             bool hl = false, hr = false;
-            uint32_t c0 = 0, c1 = 0;
+            uint32_t c0 = 0, c1 = 0, seg = 0;
             if (base + lane < nf) {
-                const NodeView nv = load_node(nodes, node_idx(front[cur * kFront + base + lane]));
-                float rl, rr;
-                hl = slab_hit(a, inv, nv.lo0 - R, nv.hi0 + R, 1.0f, &rl);
-                hr = slab_hit(a, inv, nv.lo1 - R, nv.hi1 + R, 1.0f, &rr);
+                const uint32_t e = front[cur * kFront + base + lane];
+                seg = e >> kSegShift;
+                const NodeView nv = load_node(nodes, e & kIdxMask);
+                const float3 sa = pick3<NS>(a, seg), si = pick3<NS>(inv, seg);
+                const float rr = pick1<NS>(r, seg);
+                const float3 R = mk3(rr, rr, rr);
+                float tl, tr;
+                hl = slab_hit(sa, si, nv.lo0 - R, nv.hi0 + R, 1.0f, &tl);
+                hr = slab_hit(sa, si, nv.lo1 - R, nv.hi1 + R, 1.0f, &tr);
                 c0 = nv.c0;
                 c1 = nv.c1;
             }
+            const uint32_t tag = seg << kSegShift;
             const uint32_t leaf0 = __ballot_sync(0xFFFFFFFFu, hl && is_leaf(c0));
             const uint32_t leaf1 = __ballot_sync(0xFFFFFFFFu, hr && is_leaf(c1));
             const uint32_t in0 = __ballot_sync(0xFFFFFFFFu, hl && !is_leaf(c0));
@@ -220,10 +260,10 @@ PZ_D int fat_query(const Node* __restrict__ nodes, uint32_t root, float3 a, floa
             const int nLeaf = __popc(leaf0) + __popc(leaf1), nIn = __popc(in0) + __popc(in1);
             if (n + nLeaf > kMaxCand || nNext + nIn > kFront) return -1;
             uint32_t* next = front + (cur ^ 1) * kFront;
-            if ((leaf0 >> lane) & 1u) cand[n + __popc(leaf0 & lt)] = node_idx(c0);
-            if ((leaf1 >> lane) & 1u) cand[n + __popc(leaf0) + __popc(leaf1 & lt)] = node_idx(c1);
-            if ((in0 >> lane) & 1u) next[nNext + __popc(in0 & lt)] = c0;
-            if ((in1 >> lane) & 1u) next[nNext + __popc(in0) + __popc(in1 & lt)] = c1;
+            if ((leaf0 >> lane) & 1u) cand[n + __popc(leaf0 & lt)] = node_idx(c0) | tag;
+            if ((leaf1 >> lane) & 1u) cand[n + __popc(leaf0) + __popc(leaf1 & lt)] = node_idx(c1) | tag;
+            if ((in0 >> lane) & 1u) next[nNext + __popc(in0 & lt)] = node_idx(c0) | tag;
+            if ((in1 >> lane) & 1u) next[nNext + __popc(in0) + __popc(in1 & lt)] = node_idx(c1) | tag;
             n += nLeaf;
             nNext += nIn;
         }
@@ -753,7 +793,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_p2_solve(BatchArgs a
 }
 
 template <int K, bool kMulti>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_p2_vis(BatchArgs a)
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 3) k_p2_vis(BatchArgs a)
 {
     __shared__ uint32_t cand[kWarpsPerBlock][kMaxCand];
     __shared__ uint32_t front[kWarpsPerBlock][2 * kFront];
@@ -786,35 +826,51 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_p2_vis(BatchArgs a)
 #pragma unroll
             for (int i = 0; i < 2 * K; i++) xs[i] = e.x[i];
         }
-        // one fattened query per path segment, shared by the block's roots; the segment
-        // endpoints are the chain's vertices and shading normals (contributableThroughput,
-        // pk.h:763-789)
-        for (int s = 0; s < K + 1; s++) {
-            const uint32_t valid = __ballot_sync(0xFFFFFFFFu, thr > 0.0f);
-            if (!valid) break;
+        // the shadow segments of every root: endpoints are the chain's vertices and shading
+        // normals (contributableThroughput, pk.h:763-789), offset as occluded() does
+        constexpr int NS = K + 1;
+        float3 sa[NS], sd[NS];
+#pragma unroll
+        for (int sg = 0; sg < NS; sg++) sa[sg] = sd[sg] = mk3(0.f, 0.f, 0.f);
+        if (thr > 0.0f) {
+            float3 va, na;
+            chain_vertex<K>(ch, xs, S.p_light, pe, 0, va, na);
+#pragma unroll
+            for (int sg = 0; sg < NS; sg++) {
+                float3 vb, nb, b;
+                chain_vertex<K>(ch, xs, S.p_light, pe, sg + 1, vb, nb);
+                shadow_segment(va, na, vb, nb, sa[sg], b);
+                sd[sg] = ex::sub3(b, sa[sg]);
+                va = vb;
+                na = nb;
+            }
+        }
+        const uint32_t valid = __ballot_sync(0xFFFFFFFFu, thr > 0.0f);
+        if (valid) {
+            // one merged query for all segments, each fattened to cover every root's segment
             const int leader = __ffs(valid) - 1;
-            float3 sa = mk3(0.f, 0.f, 0.f), sb = mk3(0.f, 0.f, 0.f);
-            if (thr > 0.0f) {
-                float3 va, na, vb, nb;
-                chain_vertex<K>(ch, xs, S.p_light, pe, s, va, na);
-                chain_vertex<K>(ch, xs, S.p_light, pe, s + 1, vb, nb);
-                shadow_segment(va, na, vb, nb, sa, sb);
+            float3 ra[NS], rinv[NS];
+            float rad[NS];
+#pragma unroll
+            for (int sg = 0; sg < NS; sg++) {
+                ra[sg] = mk3(__shfl_sync(0xFFFFFFFFu, sa[sg].x, leader), __shfl_sync(0xFFFFFFFFu, sa[sg].y, leader),
+                             __shfl_sync(0xFFFFFFFFu, sa[sg].z, leader));
+                const float3 rd = mk3(__shfl_sync(0xFFFFFFFFu, sd[sg].x, leader),
+                                      __shfl_sync(0xFFFFFFFFu, sd[sg].y, leader),
+                                      __shfl_sync(0xFFFFFFFFu, sd[sg].z, leader));
+                const float3 rb = ra[sg] + rd;
+                rinv[sg] = inv_rd(rb - ra[sg]);
+                float dev = 0.0f, mag = 0.0f;
+                if (thr > 0.0f) {
+                    const float3 da = vabs(sa[sg] - ra[sg]), db = vabs((sa[sg] + sd[sg]) - rb);
+                    dev = fmaxf(fmaxf(fmaxf(da.x, da.y), da.z), fmaxf(fmaxf(db.x, db.y), db.z));
+                    const float3 ma = vabs(sa[sg]), mb = vabs(sa[sg] + sd[sg]);
+                    mag = fmaxf(fmaxf(fmaxf(ma.x, ma.y), ma.z), fmaxf(fmaxf(mb.x, mb.y), mb.z));
+                }
+                // covers the rounding of the slab and box arithmetic
+                rad[sg] = warp_max(dev) + 1.0e-5f * (1.0f + warp_max(mag));
             }
-            const float3 ra = mk3(__shfl_sync(0xFFFFFFFFu, sa.x, leader), __shfl_sync(0xFFFFFFFFu, sa.y, leader),
-                                  __shfl_sync(0xFFFFFFFFu, sa.z, leader));
-            const float3 rb = mk3(__shfl_sync(0xFFFFFFFFu, sb.x, leader), __shfl_sync(0xFFFFFFFFu, sb.y, leader),
-                                  __shfl_sync(0xFFFFFFFFu, sb.z, leader));
-            float rad = 0.0f, mag = 0.0f;
-            if (thr > 0.0f) {
-                const float3 da = vabs(sa - ra), db = vabs(sb - rb);
-                rad = fmaxf(fmaxf(fmaxf(da.x, da.y), da.z), fmaxf(fmaxf(db.x, db.y), db.z));
-                const float3 ma = vabs(sa), mb = vabs(sb);
-                mag = fmaxf(fmaxf(fmaxf(ma.x, ma.y), ma.z), fmaxf(fmaxf(mb.x, mb.y), mb.z));
-            }
-            rad = warp_max(rad);
-            mag = warp_max(mag);
-            rad += 1.0e-5f * (1.0f + mag);  // covers the rounding of the slab and box arithmetic
-            const int nc = fat_query(S.nodes, root, ra, rb, rad, cand[warp], front[warp]);
+            const int nc = fat_query_multi<NS>(S.nodes, root, ra, rinv, rad, (1u << NS) - 1u, cand[warp], front[warp]);
             __syncwarp();
             if (lane == 0) {
                 cQueries++;
@@ -822,17 +878,22 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_p2_vis(BatchArgs a)
                 else cCand += (unsigned long long)nc;
             }
             if (thr > 0.0f) {
-                const float3 d = ex::sub3(sb, sa);
                 bool occ = false;
                 if (nc < 0) {
-                    occ = any_hit(S.nodes, S.tris, root, sa, d, 1.0f) < 1.0f;
+#pragma unroll 1
+                    for (int sg = 0; sg < NS && !occ; sg++)
+                        occ = any_hit(S.nodes, S.tris, root, pick3<NS>(sa, sg), pick3<NS>(sd, sg), 1.0f) < 1.0f;
                 } else {
                     for (int c = 0; c < nc && !occ; c++) {
+                        const uint32_t e = cand[warp][c];
+                        const uint32_t sg = e >> kSegShift;
                         float3 v0, v1, v2;
-                        load_tri(S.tris, cand[warp][c], v0, v1, v2);
+                        load_tri(S.tris, e & kIdxMask, v0, v1, v2);
                         float t, u, v;
                         float3 ng;
-                        if (ray_triangle(&t, &u, &v, &ng, 0.0f, 1.0f, sa, d, v0, v1, v2) && t < 1.0f) occ = true;
+                        if (ray_triangle(&t, &u, &v, &ng, 0.0f, 1.0f, pick3<NS>(sa, sg), pick3<NS>(sd, sg), v0, v1, v2) &&
+                            t < 1.0f)
+                            occ = true;
                     }
                 }
                 if (occ) thr = 0.0f;
@@ -890,7 +951,7 @@ static cudaError_t launch_phases(const BatchArgs& a, int blocksPerSM, int p1Bloc
         cudaError_t e = cudaMemsetAsync(a.p2, 0, 4 * sizeof(unsigned long long), s);
         if (e != cudaSuccess) return e;
         k_p2_solve<K, kMulti><<<sms * blocksPerSM, kWarpsPerBlock * 32, 0, s>>>(a);
-        k_p2_vis<K, kMulti><<<sms * 4, kWarpsPerBlock * 32, 0, s>>>(a);
+        k_p2_vis<K, kMulti><<<sms * 3, kWarpsPerBlock * 32, 0, s>>>(a);
         k_p2_contrib<K, kMulti><<<sms * 8, 256, 0, s>>>(a);
     }
     return cudaGetLastError();

@@ -39,20 +39,6 @@ inline int num_sms()
     return v;
 }
 
-// Once per (kernel, device) flag for host set-up such as cudaFuncSetAttribute, whose
-// effect is per device: the caller passes a kMaxDevices array owned by the kernel.
-inline bool first_on_device(std::atomic<bool> (&done)[kMaxDevices])
-{
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return true;
-    return !done[dev].load(std::memory_order_acquire);
-}
-inline void mark_done_on_device(std::atomic<bool> (&done)[kMaxDevices])
-{
-    int dev = 0;
-    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxDevices) done[dev].store(true, std::memory_order_release);
-}
-
 struct Tri { float3 v0, v1, v2; };                        // 36 B, minimum_lbvh.h:207
 struct Attrib { int32_t material; float3 n0, n1, n2; };   // 40 B, pk.h:74
 struct Box { float3 lo, hi; };                            // 24 B, minimum_lbvh.h:220

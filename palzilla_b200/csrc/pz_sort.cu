@@ -306,14 +306,12 @@ static cudaError_t launch_pass(const KeyT* kin, KeyT* kout, const uint32_t* vin,
                                int pass, Header* h, unsigned long long* lookback, cudaStream_t s)
 {
     const size_t smem = sizeof(PassSmem<KeyT, kHasVal>);
-    // the shared-memory limit is an attribute of the function on each device: set it once per device
-    static std::atomic<bool> configured[kMaxDevices];
-    if (first_on_device(configured)) {
-        cudaError_t e = cudaFuncSetAttribute(k_pass<KeyT, kHasVal>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-        mark_done_on_device(configured);
-    }
+    // The shared-memory limit above 48 KB is an attribute of the function in each CUDA context (the
+    // module is loaded per context), so it is set before every launch: a flag per device or per
+    // context handle would miss a context created after the first call, or one re-created at the
+    // same address.  Setting it again is a cheap host call and changes nothing.
+    cudaError_t e = cudaFuncSetAttribute(k_pass<KeyT, kHasVal>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     k_pass<KeyT, kHasVal><<<num_tiles(n), kThreads, smem, s>>>(kin, kout, vin, vout, n, bit, pass, h, lookback);
     return cudaGetLastError();
 }
