@@ -336,11 +336,13 @@ __device__ __noinline__ float dadw_out_of_line(const Chain<K>& ch, const float* 
 template <int K>
 __device__ __noinline__ bool newton_nl(float* x, const Chain<K>& ch, float3 p_light, float3 p, float eta,
                                        uint32_t events, int maxIterations, float tol, int warmup, bool edge,
-                                       int minSteps, float* det)
+                                       int minSteps, float* det, int* itersOut = nullptr)
 {
     int it;
-    return newton<float, K>(x, v3f<float>(p_light), v3f<float>(p), ch, eta, events, maxIterations, tol, warmup, edge,
-                            &it, det, minSteps);
+    const bool c = newton<float, K>(x, v3f<float>(p_light), v3f<float>(p), ch, eta, events, maxIterations, tol, warmup,
+                                    edge, &it, det, minSteps);
+    if (itersOut) *itersOut = it;
+    return c;
 }
 
 // The plain path's solve (solveConstraints' rules from the photon's start: cost tolerance,
@@ -689,7 +691,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_p2_solve(BatchArgs a
     unsigned long long* const nAccepted = a.p2 + 0;
     unsigned long long* const nBlocks = a.p2 + 1;
     unsigned long long* const reserved = a.p2 + 2;
-    unsigned long long nConv = 0, cNewton = 0, cPolish = 0;
+    unsigned long long nConv = 0, cNewton = 0, cPolish = 0, cIters = 0, cWarm = 0;
     for (;;) {
         // one record per queue access, after reserving room for its accepted roots in this wave
         unsigned long long j = 0;
@@ -737,11 +739,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_p2_solve(BatchArgs a
                     for (int i = 0; i < 2 * K; i++) xs[i] = x0[i];
                 }
                 float det = 1.0f;
+                int its = 0;
                 // a predicted root is refined by Newton; every other bin runs the plain path's
                 // solver from the photon's start, so its accept / reject decision is the plain one
                 const bool conv = newton_nl<K>(xs, ch, S.p_light, pe, eta, S.events, S.maxIterations,
-                                               S.costTolerance, S.earlyTermWarmUp, true, warm ? 1 : 0, &det);
+                                               S.costTolerance, S.earlyTermWarmUp, true, warm ? 1 : 0, &det, &its);
                 cNewton++;
+                cIters += its;
+                cWarm += warm;
                 if (conv && S.roots) {
                     float* rt = S.roots + ((size_t)r.item * B + b) * 8;
 #pragma unroll
@@ -789,6 +794,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_p2_solve(BatchArgs a
     if (a.counters) {
         flush_count(a.counters + kCntNewton2, cNewton);
         flush_count(a.counters + kCntPolish, cPolish);
+        flush_count(a.counters + kCntNewtonIters, cIters);
+        flush_count(a.counters + kCntWarm, cWarm);
     }
 }
 

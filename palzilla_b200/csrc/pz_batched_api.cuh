@@ -30,7 +30,8 @@ struct BatchArgs {
     unsigned long long acceptCapacity = 0;
     void* blocks = nullptr;            // blockCapacity entries of block_bytes()
     unsigned long long blockCapacity = 0;
-    unsigned long long* p2 = nullptr;  // device u64[4]: accepted count, block count, reserved, blocks taken
+    unsigned long long* p2 = nullptr;  // device u64[4] (scratch header byte 192): accepted count, block count,
+                                       // reserved, blocks taken
 };
 
 // Phase 2 runs in at most kMaxWaves waves; each wave has room for 64 accepted roots (a record's
@@ -55,7 +56,7 @@ struct SceneArgs {
 // diagnostics counters
 enum {
     kCntMode0 = 0, kCntMode1, kCntMode2, kCntNewton2, kCntPolish, kCntFatOverflow, kCntCandidates, kCntQueries,
-    kCntFallbackNoConv, kCntFallbackShift, kCntFallbackProbe, kNumCounters
+    kCntFallbackNoConv, kCntFallbackShift, kCntFallbackProbe, kCntNewtonIters, kCntWarm, kNumCounters
 };
 
 // bytes of one phase-1 record for chain length K

@@ -275,9 +275,9 @@ extern "C" int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32
     b.acceptCapacity = batched::accept_capacity(desc->n_paths);
     b.blocks = base + L.blocks;
     b.blockCapacity = batched::block_capacity(desc->n_paths);
-    b.p2 = reinterpret_cast<unsigned long long*>(base + 160);
+    b.p2 = reinterpret_cast<unsigned long long*>(base + 192);
     b.nPathsDev = n_paths_dev;
-    static_assert(64 + 8 * batched::kNumCounters <= 256, "counters live in the 256-byte scratch header");
+    static_assert(64 + 8 * batched::kNumCounters <= 192, "counters live in the scratch header before the phase-2 words");
     b.counters = reinterpret_cast<unsigned long long*>(base + 64);
     b.polishDet = desc->polish_det > 0.0f ? (double)desc->polish_det : 0.0;
     b.grazeCos = desc->graze_cos > 0.0f ? desc->graze_cos : 0.0f;
@@ -401,7 +401,7 @@ static int multi_args(int K, int n_bins, uint32_t n_scenes, uint64_t total, void
     b->acceptCapacity = batched::accept_capacity(total);
     b->blocks = base + L.blocks;
     b->blockCapacity = batched::block_capacity(total);
-    b->p2 = reinterpret_cast<unsigned long long*>(base + 160);
+    b->p2 = reinterpret_cast<unsigned long long*>(base + 192);
     b->polishDet = 0.0;
     b->grazeCos = 0.0f;
     b->continuation = 0;

@@ -226,25 +226,40 @@ PZ_D void pass_tile(PassSmem<KeyT, kHasVal>& S, const KeyT* __restrict__ kin, Ke
         }
     }
 
-    // ---- decoupled look-back over earlier tiles for digit d
+    // ---- decoupled look-back over earlier tiles for digit d.  The words of kLookBatch
+    //      predecessors are loaded at once (independent loads in flight, each a coalesced row
+    //      across the block's digit threads), then consumed in order: aggregates are added up
+    //      to the first inclusive prefix; a word not yet published ends the batch, and the
+    //      next batch starts at it.  Tile 0 publishes its prefix at once, so every walk ends.
     if (d < kRadix) {
         uint32_t prefix = 0;
         if (tile != 0) {
             int t = (int)tile - 1;
             uint32_t spins = 0;
-            while (t >= 0) {
-                const unsigned long long w = ld_volatile(lookback + (size_t)t * kRadix + d);
-                if ((w & ~0x3FFFFFFFFull) != tag || (w & (3ull << 32)) == 0) {
+            bool done = false;
+            while (!done) {
+                unsigned long long w[kLookBatch];
+#pragma unroll
+                for (int j = 0; j < kLookBatch; j++)
+                    w[j] = t - j >= 0 ? ld_volatile(lookback + (size_t)(t - j) * kRadix + d) : 0ull;
+                int used = 0;
+#pragma unroll
+                for (int j = 0; j < kLookBatch; j++) {
+                    if (done || used != j) break;
+                    const unsigned long long x = w[j];
+                    if ((x & ~0x3FFFFFFFFull) != tag || (x & (3ull << 32)) == 0) break;  // not yet published
+                    prefix += (uint32_t)x;
+                    used = j + 1;
+                    if (x & kFlagP) done = true;
+                }
+                t -= used;
+                if (!done && used == 0) {
                     if (++spins > kSpinLimit) {
                         raise_error(&h->status, kErrSpinLimit);
                         break;
                     }
                     if (spins > 16) __nanosleep(32);
-                    continue;
                 }
-                prefix += (uint32_t)w;
-                if (w & kFlagP) break;
-                t--;
             }
             st_volatile(mine, tag | kFlagP | (uint32_t)(prefix + total));
         }

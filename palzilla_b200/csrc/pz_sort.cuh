@@ -10,11 +10,13 @@
 // Design (independent of the reference's kernels):
 //  * one histogram kernel computes every pass's digit counts in a single read and,
 //    in the same launch, clears the look-back table;
-//  * one kernel per pass: tiles of 4096 items claim a tile index from an atomic
-//    counter (so a tile only ever waits on tiles that are already running), rank
-//    keys stably with warp ballots, resolve the tile's global digit offsets with a
-//    decoupled look-back over 64-bit words {value, flag, pass tag}, stage the tile
-//    in shared memory in digit order and write digit runs out coalesced;
+//  * one kernel per pass: tiles of kThreads x kItems items claim a tile index from an
+//    atomic counter (so a tile only ever waits on tiles that are already running), count
+//    digits per warp and publish the tile's aggregate before ranking, rank keys stably
+//    from per-warp digit masks in shared memory, resolve the tile's global digit offsets
+//    with a decoupled look-back over 64-bit words {value, flag, pass tag} that loads
+//    kLookBatch predecessors at a time, stage the tile in shared memory in digit order and
+//    write digit runs out coalesced;
 //  * every spin wait is bounded; on expiry the kernel sets kErrSpinLimit in the
 //    status word and finishes (with undefined output) instead of hanging.
 #pragma once
@@ -56,6 +58,10 @@ constexpr int kRadix = 256;
 constexpr int kMaxPasses = 8;
 constexpr int kHistBlocksPerSM = 4;
 constexpr uint32_t kSpinLimit = 1u << 22;
+#ifndef PZ_SORT_LOOK_BATCH
+#define PZ_SORT_LOOK_BATCH 8
+#endif
+constexpr int kLookBatch = PZ_SORT_LOOK_BATCH;  // predecessor words a look-back step loads at once
 
 // Scratch header (the first kHeaderBytes of the sort scratch).
 struct Header {
