@@ -169,17 +169,24 @@ PZ_API int pz_photon_trace(const pz_internal_node* internals_dev, const uint32_t
 typedef struct pz_ray_generator { pz_float3 origin, right, up; } pz_ray_generator; /* RayGenerator, camera.h:4-41 */
 typedef struct pz_lens_params { float distance, thickness, R; } pz_lens_params;   /* LensParams, pk.h:1035-1040 */
 typedef struct pz_first_diffuse { pz_float3 p, ng, R; float lambda; } pz_first_diffuse; /* FirstDiffuse, pk.h:80-86 */
+/* Texture8RGBX (pk.h:1075-1098): an 8-bit RGBX image (4 bytes per texel, row-major, width x
+ * height) in device memory, sampled at the receiver point (x, z) with repeat wrapping and the
+ * nearest texel, each channel decoded as (c / 255)^2.2. */
+typedef struct pz_texture_rgbx { const uint8_t* texels_dev; uint32_t width, height; } pz_texture_rgbx;
 /* RayGenerator::lookat (camera.h:10-22), on the host. */
 PZ_API void pz_ray_generator_lookat(pz_ray_generator* gen, pz_float3 eye, pz_float3 center, pz_float3 up, float fovy,
                                     int width, int height);
 /* solvePrimary (main_gpu.cu:213-371).  accum_dev: 4 floats per pixel (RGB + sample
- * count), added to.  The receiver albedo is a constant; lens->R <= 0 disables the lens. */
+ * count), added to.  The albedo of a diffuse hit is the floor texture sampled at the hit's
+ * (x, z) as the reference samples it (main_gpu.cu:343), or the constant `albedo` when
+ * albedo_texture is NULL; lens->R <= 0 disables the thick lens (pk.h:1042-1073). */
 PZ_API int pz_solve_primary(float* accum_dev, pz_first_diffuse* first_diffuse_dev, int width, int height,
                             const pz_ray_generator* gen, const pz_lens_params* lens,
                             const pz_internal_node* internals_dev, const uint32_t* root_dev,
                             const pz_triangle* triangles_dev, const pz_triangle_attrib* attribs_dev, pz_float3 p_light,
                             float light_intensity, float radiance_clamp, float cauchy_a, float cauchy_b,
-                            pz_float3 albedo, int iteration, uint32_t* status_dev, pz_stream_t stream);
+                            pz_float3 albedo, const pz_texture_rgbx* albedo_texture, int iteration,
+                            uint32_t* status_dev, pz_stream_t stream);
 
 /* ---------------------------------------------------------------- (pixel, tuple) work list */
 typedef struct pz_specular_path { int32_t pixel; int32_t cache_index; } pz_specular_path; /* pk.h:1102-1106 */

@@ -204,6 +204,21 @@ public:
         check_cuda(cudaSetDevice(device), "PKRenderer::setup");
         m_onesweep = OnesweepSort(device);
     }
+    // Floor texture (the reference's Texture8RGBX, pk.h:1075-1098, loaded from an image file at
+    // setup): RGBX texels, row-major, width x height, sampled at a diffuse hit's (x, z).  An
+    // empty vector removes it (the diffuse hits then take m_albedo).
+    void setFloorTexture(const std::vector<uint8_t>& rgbx, int width, int height)
+    {
+        if (rgbx.empty()) {
+            m_floorTexture.release();
+            return;
+        }
+        if (width <= 0 || height <= 0 || rgbx.size() != (size_t)width * height * 4)
+            throw Error(PZ_ERR_INVALID_ARGUMENT, "setFloorTexture: size mismatch");
+        m_floorTexture.upload(rgbx);
+        m_floorTextureSize[0] = width;
+        m_floorTextureSize[1] = height;
+    }
     // Scene from arrays (the reference reads an Alembic frame, pk.h:1246-1366).
     void loadFrame(const std::vector<pz_triangle>& triangles, const std::vector<pz_triangle_attrib>& attribs)
     {
@@ -238,11 +253,13 @@ public:
         cudaStream_t s = 0;
         const int n = m_gpuBuilder.m_nTriangles;
         m_lightPoint = light_point(m_p_light, m_lightSize[0], m_lightSize[1], m_iteration);
+        const pz_texture_rgbx floor = {m_floorTexture.data(), (uint32_t)m_floorTextureSize[0],
+                                       (uint32_t)m_floorTextureSize[1]};
         check(pz_solve_primary(m_accumulators.data(), m_firstDiffuses.data(), m_imageWidth, m_imageHeight, &m_camera.g,
                                &m_lensParams, m_gpuBuilder.m_internals, m_gpuBuilder.m_rootNode,
                                m_trianglesDevice.data(), m_triangleAttribsDevice.data(), m_lightPoint, m_lightIntencity,
-                               m_radianceClamp, m_cauchyA, m_cauchyB, m_albedo, m_iteration, m_status.data(),
-                               (pz_stream_t)s),
+                               m_radianceClamp, m_cauchyA, m_cauchyB, m_albedo, m_floorTexture.data() ? &floor : nullptr,
+                               m_iteration, m_status.data(), (pz_stream_t)s),
               "solvePrimary");
         check(pz_path_cache_clear(m_pathCache.data(), kPathCacheCapacity, (pz_stream_t)s), "PathCache::clear");
         // eta at the two ends of the visible band, 380 and 780 nm (pk.h:1448-1449)
@@ -327,6 +344,8 @@ private:
 
     OnesweepSort m_onesweep;
     BVHGPUBuilder m_gpuBuilder;
+    DeviceBuffer<uint8_t> m_floorTexture;
+    int m_floorTextureSize[2] = {0, 0};
     DeviceBuffer<pz_triangle> m_trianglesDevice;
     DeviceBuffer<pz_triangle_attrib> m_triangleAttribsDevice;
     DeviceBuffer<uint8_t> m_pathCache;

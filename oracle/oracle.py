@@ -208,16 +208,21 @@ class CpuLib:
                          _p(np.asarray(up, np.float32)), C.c_float(fovy), C.c_int(w), C.c_int(h), _p(out))
         return out
 
-    def solve_primary(self, bvh, scene, ray_gen, iteration=0, lens=(0.6, 0.05, 0.0)):
+    def solve_primary(self, bvh, scene, ray_gen, iteration=0, lens=(0.6, 0.05, 0.0), texture=None):
+        """solvePrimary (main_gpu.cu:213-371); texture: an optional floor texture, uint8 array
+        (height, width, 4), sampled as Texture8RGBX (pk.h:1075-1098)."""
         W, H = scene.width, scene.height
         accum = np.zeros((H * W, 4), np.float32)
         fd = np.zeros((H * W, 10), np.float32)
+        tex = None if texture is None else np.ascontiguousarray(texture, np.uint8)
         self.f("solve_primary")(_p(accum), _p(fd), C.c_int(W), C.c_int(H), _p(np.asarray(ray_gen, np.float32)),
                                 _p(np.asarray(lens, np.float32)), _p(bvh["nodes"]), C.c_uint32(bvh["root"]),
                                 _p(scene.tris), _p(scene.attribs), _p(_light(scene, iteration)),
                                 C.c_float(scene.light_intensity), C.c_float(scene.radiance_clamp),
                                 C.c_float(scene.cauchy_a), C.c_float(scene.cauchy_b),
-                                _p(np.asarray(scene.albedo, np.float32)), C.c_int(iteration))
+                                _p(np.asarray(scene.albedo, np.float32)), _p(tex),
+                                C.c_int(0 if tex is None else tex.shape[1]), C.c_int(0 if tex is None else tex.shape[0]),
+                                C.c_int(iteration))
         return accum, fd
 
     # ------------------------------------------------------------------ solver primitives

@@ -230,17 +230,31 @@ void pzo_lookat(const float* eye, const float* center, const float* up, float fo
     st3(out9 + 6, g.up);
 }
 
-// solvePrimary (main_gpu.cu:213-371) with a constant receiver albedo in place of the
-// floor texture and the thick lens applied only when lensR > 0.
+// Texture8RGBX::samplePoint (pk.h:1083-1095): repeat wrapping, nearest texel, each channel
+// decoded as (c / 255)^2.2.
+static F3 sample_point(const uint8_t* tex, int tw, int th, float u, float v)
+{
+    u = u - std::floor(u);
+    v = v - std::floor(v);
+    const int ix = (int)std::fmin(u * (float)tw, (float)tw - 1.0f);
+    const int iy = (int)std::fmin(v * (float)th, (float)th - 1.0f);
+    const uint8_t* c = tex + 4 * ((size_t)ix + (size_t)tw * iy);
+    return mk(std::pow((float)c[0] / 255.0f, 2.2f), std::pow((float)c[1] / 255.0f, 2.2f),
+              std::pow((float)c[2] / 255.0f, 2.2f));
+}
+
+// solvePrimary (main_gpu.cu:213-371): the thick lens applied only when lensR > 0, and the
+// diffuse hit's albedo from the floor texture tex (RGBX, tw x th) sampled at its (x, z), or
+// the constant albedo3 when tex is null.
 // out: firstDiffuse as 10 floats per pixel {p, ng, R, lambda}; accum 4 floats per pixel (added).
 void pzo_solve_primary(float* accum, float* firstDiffuse, int W, int H, const float* rayGen9, const float* lens3,
                        const InternalNode* nodes, uint32_t root, const Triangle* tris, const TriangleAttrib* attribs,
                        const float* p_light, float lightIntensity, float radianceClamp, float cauchyA, float cauchyB,
-                       const float* albedo3, int iteration)
+                       const float* albedo3, const uint8_t* tex, int tw, int th, int iteration)
 {
     RayGenerator g{ld3(rayGen9), ld3(rayGen9 + 3), ld3(rayGen9 + 6)};
     F3 L = ld3(p_light);
-    F3 albedo = ld3(albedo3);
+    const F3 albedoConst = ld3(albedo3);
 #pragma omp parallel for schedule(dynamic, 4)
     for (int yi = 0; yi < H; yi++) {
         for (int xi = 0; xi < W; xi++) {
@@ -318,6 +332,7 @@ void pzo_solve_primary(float* accum, float* firstDiffuse, int W, int H, const fl
             if (0.0f < dot(n, rd)) n = -n;
             F3 toL = L - p;
             float d2 = dot(toL, toL);
+            const F3 albedo = tex ? sample_point(tex, tw, th, p.x, p.z) : albedoConst;
             F3 Lr = mk(0.f, 0.f, 0.f);
             if (!occluded(nodes, tris, root, p, n, L, mk(0.f, 0.f, 0.f))) {
                 float contrib = lightIntensity / d2 * std::fmax(dot(normalize(toL), n), 0.0f);

@@ -34,6 +34,10 @@ class LensParams(C.Structure):
     _fields_ = [("distance", f32), ("thickness", f32), ("R", f32)]
 
 
+class TextureRGBX(C.Structure):
+    _fields_ = [("texels_dev", C.c_void_p), ("width", C.c_uint32), ("height", C.c_uint32)]
+
+
 class BatchTuning(C.Structure):
     _fields_ = [("p1_blocks_per_sm", C.c_int), ("p2_blocks_per_sm", C.c_int), ("p2_chunk", C.c_int)]
 
@@ -82,7 +86,7 @@ SIGNATURES = {
     "pz_photon_trace": (i32, [vp, vp, vp, vp, i32, i32, Float3, f32, f32, i32, f32, vp, u32, f32, vp, vp]),
     "pz_ray_generator_lookat": (None, [C.POINTER(RayGenerator), Float3, Float3, Float3, f32, i32, i32]),
     "pz_solve_primary": (i32, [vp, vp, i32, i32, C.POINTER(RayGenerator), C.POINTER(LensParams), vp, vp, vp, vp,
-                               Float3, f32, f32, f32, f32, Float3, i32, vp, vp]),
+                               Float3, f32, f32, f32, f32, Float3, C.POINTER(TextureRGBX), i32, vp, vp]),
     "pz_lookup_flatten": (i32, [u32, vp, vp, vp, u32, vp, i32, vp, u32, f32, vp]),
     "pz_reorder_specular_paths": (i32, [vp, vp, vp, u32, vp]),
     "pz_solve_specular_plain": (i32, [C.POINTER(SolveDesc), vp]),

@@ -233,17 +233,25 @@ class Frame:
         self.iteration = 0  # the iteration of the last eye pass (its light point)
 
 
-def solve_primary(ds: DeviceScene, frame: Frame, iteration: int = 0, lens=(0.6, 0.05, 0.0), stream=None):
+def solve_primary(ds: DeviceScene, frame: Frame, iteration: int = 0, lens=(0.6, 0.05, 0.0), texture=None,
+                  stream=None):
+    """solvePrimary (main_gpu.cu:213-371).  texture: an optional floor texture, a uint8 cuda
+    tensor of shape (height, width, 4) (RGBX), sampled at the diffuse hit's (x, z) as
+    Texture8RGBX (pk.h:1075-1098); None = the scene's constant albedo."""
     sc = ds.scene
     frame.iteration = iteration
     g = ray_generator(sc)
     l = _lib.LensParams(*[float(x) for x in lens])
+    tex = None
+    if texture is not None:
+        assert texture.dtype == torch.uint8 and texture.dim() == 3 and texture.shape[2] == 4 and texture.is_contiguous()
+        tex = _lib.TextureRGBX(texture.data_ptr(), int(texture.shape[1]), int(texture.shape[0]))
     _lib.call("pz_solve_primary", _vp(frame.accum), _vp(frame.fd), C.c_int(sc.width), C.c_int(sc.height), C.byref(g),
               C.byref(l), _vp(ds.internals), _vp(ds.root_dev), _vp(ds.tris), _vp(ds.attribs),
               _lib.f3(sc.light_point(iteration)),
               C.c_float(sc.light_intensity), C.c_float(sc.radiance_clamp), C.c_float(sc.cauchy_a),
-              C.c_float(sc.cauchy_b), _lib.f3(sc.albedo), C.c_int(iteration), _vp(frame.status),
-              C.c_void_p(_stream(stream)))
+              C.c_float(sc.cauchy_b), _lib.f3(sc.albedo), C.byref(tex) if tex is not None else None, C.c_int(iteration),
+              _vp(frame.status), C.c_void_p(_stream(stream)))
 
 
 def lookup_flatten(frame: Frame, cache: PathCache, events: int, stream=None) -> int:

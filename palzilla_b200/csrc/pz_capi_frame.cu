@@ -129,20 +129,28 @@ extern "C" int pz_solve_primary(float* accum_dev, pz_first_diffuse* first_diffus
                                 const pz_internal_node* internals_dev, const uint32_t* root_dev,
                                 const pz_triangle* triangles_dev, const pz_triangle_attrib* attribs_dev,
                                 pz_float3 p_light, float light_intensity, float radiance_clamp, float cauchy_a,
-                                float cauchy_b, pz_float3 albedo, int iteration, uint32_t* status_dev,
-                                pz_stream_t stream)
+                                float cauchy_b, pz_float3 albedo, const pz_texture_rgbx* albedo_texture,
+                                int iteration, uint32_t* status_dev, pz_stream_t stream)
 {
     if (width < 0 || height < 0 || !gen || !accum_dev || !first_diffuse_dev || !root_dev || !triangles_dev ||
         !attribs_dev)
         return fail(PZ_ERR_INVALID_ARGUMENT, "pz_solve_primary: bad argument");
+    Tex tex{nullptr, 0u, 0u};
+    if (albedo_texture) {
+        if (!albedo_texture->texels_dev || albedo_texture->width == 0 || albedo_texture->height == 0 ||
+            (reinterpret_cast<uintptr_t>(albedo_texture->texels_dev) & 3))
+            return fail(PZ_ERR_INVALID_ARGUMENT,
+                        "pz_solve_primary: the albedo texture needs texels (4-byte aligned) and a non-zero size");
+        tex = Tex{albedo_texture->texels_dev, albedo_texture->width, albedo_texture->height};
+    }
     RayGen g{F3(gen->origin), F3(gen->right), F3(gen->up)};
     Lens l{0.6f, 0.05f, 0.0f};
     if (lens) l = Lens{lens->distance, lens->thickness, lens->R};
     return done(launch_primary(reinterpret_cast<float4*>(accum_dev), reinterpret_cast<FirstDiffuse*>(first_diffuse_dev),
                                width, height, g, l, reinterpret_cast<const Node*>(internals_dev), root_dev,
                                reinterpret_cast<const Tri*>(triangles_dev), reinterpret_cast<const Attrib*>(attribs_dev),
-                               F3(p_light), light_intensity, radiance_clamp, cauchy_a, cauchy_b, F3(albedo), iteration,
-                               status_dev, S(stream)),
+                               F3(p_light), light_intensity, radiance_clamp, cauchy_a, cauchy_b, F3(albedo), tex,
+                               iteration, status_dev, S(stream)),
                 "pz_solve_primary");
 }
 

@@ -4,9 +4,10 @@
 //             optional thick lens (pk.h:1042-1073), up to 32 specular bounces with
 //             Fresnel-sampled events to the first diffuse hit, point-light direct light
 //             with a shadow ray; writes FirstDiffuse {p, n, R, lambda} and adds to the
-//             float4 accumulator.  The receiver albedo is a constant (the reference
-//             samples a floor texture, pk.h:1075-1098).  Bit-exact with the CPU oracle
-//             except lambda, which goes through expf/logf.
+//             float4 accumulator.  The albedo of the diffuse hit is the floor texture sampled
+//             at its (x, z) (Texture8RGBX, pk.h:1075-1098; main_gpu.cu:343) or a constant.
+//             Bit-exact with the CPU oracle except lambda, which goes through expf/logf,
+//             and the texture's gamma decode, which goes through powf.
 // k_lookup:   lookupFlatten (main_gpu.cu:373-416): per pixel, the PathCache slots of the
 //             pixel's cell with the requested event string, appended to the work list as
 //             SpecularPath {pixel, slot} and IndexedSpecularPath {path hash, index}.
@@ -37,7 +38,8 @@ __global__ void __launch_bounds__(256) k_primary(float4* __restrict__ accum, Fir
                                                  const uint32_t* __restrict__ rootPtr, const Tri* __restrict__ tris,
                                                  const Attrib* __restrict__ attribs, float3 p_light,
                                                  float lightIntensity, float radianceClamp, float cauchyA,
-                                                 float cauchyB, float3 albedo, int iteration, uint32_t* status)
+                                                 float cauchyB, float3 albedo, Tex tex, int iteration,
+                                                 uint32_t* status)
 {
     const int xi = blockIdx.x * 16 + (threadIdx.x & 15);
     const int yi = blockIdx.y * 16 + (threadIdx.x >> 4);
@@ -135,15 +137,16 @@ __global__ void __launch_bounds__(256) k_primary(float4* __restrict__ accum, Fir
     if (0.0f < dot(n, rd)) n = -n;
     const float3 toL = p_light - p;
     const float d2 = dot(toL, toL);
+    const float3 R = tex.texels ? sample_point(tex, p.x, p.z) : albedo;
     float3 L = mk3(0.f, 0.f, 0.f);
     if (!occluded(nodes, tris, root, p, n, p_light, mk3(0.f, 0.f, 0.f))) {
         float contrib = lightIntensity / d2 * fmaxf(dot(normalize(toL), n), 0.0f);
         contrib = fminf(contrib, radianceClamp);
-        L = L + (albedo / kPi) * lambda_to_srgb(lambda) * contrib / p_lambda;
+        L = L + (R / kPi) * lambda_to_srgb(lambda) * contrib / p_lambda;
     }
     fd->p = p;
     fd->ng = n;
-    fd->R = albedo;
+    fd->R = R;
     fd->lambda = lambda;
     acc.x += L.x;
     acc.y += L.y;
@@ -201,11 +204,11 @@ __global__ void k_reorder(const unsigned long long* __restrict__ indexed, Specul
 cudaError_t launch_primary(float4* accum, FirstDiffuse* fds, int W, int H, const RayGen& g, const Lens& lens,
                            const Node* nodes, const uint32_t* root, const Tri* tris, const Attrib* attribs,
                            float3 p_light, float lightIntensity, float radianceClamp, float cauchyA, float cauchyB,
-                           float3 albedo, int iteration, uint32_t* status, cudaStream_t s)
+                           float3 albedo, const Tex& tex, int iteration, uint32_t* status, cudaStream_t s)
 {
     dim3 grid((W + 15) / 16, (H + 15) / 16);
     k_primary<<<grid, 256, 0, s>>>(accum, fds, W, H, g, lens, nodes, root, tris, attribs, p_light, lightIntensity,
-                                   radianceClamp, cauchyA, cauchyB, albedo, iteration, status);
+                                   radianceClamp, cauchyA, cauchyB, albedo, tex, iteration, status);
     return cudaGetLastError();
 }
 

@@ -362,3 +362,94 @@ def uneven_batch(n_scenes: int = 256, seed: int = 3001, side_min: int = 16, side
         s.photons_per_triangle = photons_per_triangle
         scenes.append(s)
     return scenes
+
+
+# ---------------------------------------------------------------------------------------
+# scene files
+# ---------------------------------------------------------------------------------------
+OBJ_MATERIALS = {"mirror": MATERIAL_MIRROR, "dielectric": MATERIAL_DIELECTRIC}
+
+
+def load_obj(path: str, materials: dict | None = None):
+    """A Wavefront OBJ triangle soup as (tris (n, 9) float32, attribs ATTRIB_DTYPE): the
+    same reading as palzilla_b200::loadObj (include/palzilla_b200_scene.hpp), triangle for
+    triangle.  The material of a face is the one its last `usemtl` names: "mirror" or
+    "dielectric", the reference's two tags (pk.h:1306-1318), else diffuse; `materials` maps
+    other names.  Polygons become fans (0, i, i + 1); a corner's normal index gives its
+    shading normal, and a triangle whose corners have none takes its unit geometric normal at
+    all three."""
+    mats = dict(OBJ_MATERIALS if materials is None else materials)
+    pos, nrm, tris, norms, mat = [], [], [], [], []
+    material = MATERIAL_DIFFUSE
+    f32 = np.float32
+
+    def resolve(i, n):
+        return i - 1 if i > 0 else n + i
+
+    with open(path) as fh:
+        for line_no, line in enumerate(fh, 1):
+            s = line.strip()
+            if s.startswith("v ") or s.startswith("v\t"):
+                x = s.split()[1:4]
+                pos.append([f32(t) for t in x])
+            elif s.startswith("vn ") or s.startswith("vn\t"):
+                x = s.split()[1:4]
+                nrm.append([f32(t) for t in x])
+            elif s.startswith("usemtl ") or s.startswith("usemtl\t"):
+                material = mats.get(s[7:].strip(), MATERIAL_DIFFUSE)
+            elif s.startswith("f ") or s.startswith("f\t"):
+                vi, ni = [], []
+                for tok in s.split()[1:]:
+                    parts = tok.split("/")
+                    v = int(parts[0])
+                    n = int(parts[2]) if len(parts) >= 3 and parts[2] else 0
+                    rv = resolve(v, len(pos))
+                    if v == 0 or not 0 <= rv < len(pos):
+                        raise ValueError(f"{path}:{line_no}: vertex index out of range")
+                    rn = -1
+                    if n != 0:
+                        rn = resolve(n, len(nrm))
+                        if not 0 <= rn < len(nrm):
+                            raise ValueError(f"{path}:{line_no}: normal index out of range")
+                    vi.append(rv)
+                    ni.append(rn)
+                if len(vi) < 3:
+                    raise ValueError(f"{path}:{line_no}: face with fewer than three corners")
+                for k in range(1, len(vi) - 1):
+                    c3 = (0, k, k + 1)
+                    t = np.array([pos[vi[c]] for c in c3], np.float32)
+                    if all(ni[c] >= 0 for c in c3):
+                        ns = np.array([nrm[ni[c]] for c in c3], np.float32)
+                    else:
+                        e0, e1 = t[1] - t[0], t[2] - t[0]
+                        g = np.array([e0[1] * e1[2] - e0[2] * e1[1], e0[2] * e1[0] - e0[0] * e1[2],
+                                      e0[0] * e1[1] - e0[1] * e1[0]], np.float32)
+                        inv = f32(1.0) / np.sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2])
+                        ns = np.tile(g * inv, (3, 1))
+                    tris.append(t.reshape(9))
+                    norms.append(ns.reshape(9))
+                    mat.append(material)
+    t = np.array(tris, np.float32).reshape(-1, 9)
+    a = np.zeros(len(mat), ATTRIB_DTYPE)
+    a["material"] = mat
+    a["ns"] = np.array(norms, np.float32).reshape(-1, 9)
+    return t, a
+
+
+def write_obj(path: str, tris: np.ndarray, attribs: np.ndarray, names=None):
+    """Writes a triangle soup as OBJ (one `v`, one `vn` per corner; `usemtl` by material:
+    names maps a material to its tag, by default the reference's "mirror" and "dielectric",
+    "diffuse" otherwise), with 9 significant digits so load_obj reads back the same float32."""
+    names = names or {MATERIAL_DIFFUSE: "diffuse", MATERIAL_MIRROR: "mirror", MATERIAL_DIELECTRIC: "dielectric"}
+    with open(path, "w") as f:
+        cur = None
+        for i in range(tris.shape[0]):
+            m = int(attribs["material"][i])
+            if m != cur:
+                f.write(f"usemtl {names[m]}\n")
+                cur = m
+            for j in range(3):
+                f.write("v %.9g %.9g %.9g\n" % tuple(float(x) for x in tris[i, 3 * j:3 * j + 3]))
+                f.write("vn %.9g %.9g %.9g\n" % tuple(float(x) for x in attribs["ns"][i, 3 * j:3 * j + 3]))
+            b = 3 * i + 1
+            f.write(f"f {b}//{b} {b + 1}//{b + 1} {b + 2}//{b + 2}\n")
