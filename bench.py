@@ -810,9 +810,63 @@ def cpu_baseline(R, seconds=15.0):
     t0 = time.perf_counter()
     _, st = lib.render_pairs(2, sel, cache, fd, bvh, sc, etas, iteration=R.iteration)
     dt = time.perf_counter() - t0
-    return {"value": float(st[0]) / dt, "unit": UNIT, "cores": lib.max_threads(), "kind": kind,
-            "sample": f"solve stage only: {len(sel)} of the frame's {n} (pixel, tuple) work items x 64 bins "
-                      f"= {int(st[0])} path solves in {dt:.1f} s"}
+    paths_per_s = float(st[0]) / dt
+    out = {"value": paths_per_s, "unit": UNIT, "cores": lib.max_threads(), "kind": kind,
+           "sample": f"solve stage: {len(sel)} of the frame's {n} (pixel, tuple) work items x 64 bins "
+                     f"= {int(st[0])} path solves in {dt:.1f} s"}
+    out["stages"] = cpu_stages(R, lib, kind, solve_paths_per_s=paths_per_s)
+    return out
+
+
+def cpu_stages(R, lib, kind, solve_paths_per_s, reps=5):
+    """The reference's CPU code per stage of the frame, median of `reps` runs each, OpenMP
+    over all host threads: BVHCPUBuilder with BUILD_OPTION_CPU_PARALLEL (minimum_lbvh.h:518-684;
+    its std::sort of the Morton keys is inside) on a 2^20-triangle soup and on the frame's
+    scene, the photon loop (photonTrace's body, main_gpu.cu:56-211) at a bounded number of
+    photons per triangle, and the eye pass (solvePrimary, main_gpu.cu:213-371; the oracle's
+    restatement); with the solve stage's paths/s, an estimate of the CPU's ms per frame."""
+    import oracle as O
+    from palzilla_b200 import scenes as S
+    sc = R.sc
+
+    def med(fn):
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            ts.append(time.perf_counter() - t0)
+        return float(np.median(ts))
+
+    soup = S.random_soup(1 << 20, seed=7)
+    cpu_parallel = 2  # BUILD_OPTION_CPU_PARALLEL
+    t_soup = med(lambda: lib.cpu_builder(soup, cpu_parallel))
+    t_scene = med(lambda: lib.cpu_builder(sc.tris, cpu_parallel))
+    b = lib.cpu_builder(sc.tris, cpu_parallel)
+    bvh = {"nodes": b["nodes"], "root": b["root"]}
+    ppt = 32
+    t_ph = med(lambda: lib.photon_trace(bvh, sc, iteration=R.iteration, photons_per_tri=ppt))
+    photons = sc.n * ppt
+    orc = O.oracle()
+    cam = sc.camera
+    gen = orc.lookat(cam.eye, cam.center, cam.up, cam.fovy, sc.width, sc.height)
+    t_eye = med(lambda: orc.solve_primary(bvh, sc, gen, iteration=R.iteration))
+    frame_photons = sc.n * sc.photons_per_triangle
+    frame_paths = float(R.n_paths) * sc.n_bins
+    ms_photon = 1e3 * t_ph * frame_photons / photons
+    ms_solve = 1e3 * frame_paths / solve_paths_per_s
+    return {
+        "cores": lib.max_threads(), "kind": kind, "reps": reps, "statistic": "median",
+        "bvh_build_2p20": {"ms": 1e3 * t_soup, "keys_per_s": (1 << 20) / t_soup,
+                           "what": "BVHCPUBuilder, BUILD_OPTION_CPU_PARALLEL, 2^20 random triangles"},
+        "bvh_build_scene": {"ms": 1e3 * t_scene, "triangles": int(sc.n)},
+        "photon_pass": {"photons_per_s": photons / t_ph, "photons": photons,
+                        "ms_at_frame_photons": ms_photon,
+                        "what": f"{ppt} photons per triangle (the frame traces {sc.photons_per_triangle})"},
+        "eye_pass": {"ms": 1e3 * t_eye, "rays_per_s": sc.width * sc.height / t_eye, "kind": "port",
+                     "what": f"{sc.width}x{sc.height} primary rays and their shadow rays"},
+        "solve": {"paths_per_s": solve_paths_per_s, "ms_at_frame_work_items": ms_solve},
+        "ms_per_frame_estimate": 1e3 * t_scene + ms_photon + 1e3 * t_eye + ms_solve,
+    }
 
 
 def run_reference(args):
