@@ -320,9 +320,10 @@ def run_ours(args):
 
     sort_build = bench_sort_build(hbm, hbm_kind) if (rank == 0 and not args.no_sort) else None
 
-    cpu = None
+    cpu = fp64 = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(R, seconds=args.cpu_seconds)
+        fp64 = fp64_error(R)
 
     if rank == 0:
         line = {
@@ -347,6 +348,7 @@ def run_ours(args):
                 frame_note="frame-level speed-up: this frame with its solve stage replaced by the reference "
                            "kernel's"),
             "image_rel_rmse": rmse,
+            "fp64_error": fp64,
             "batched_counters": counters,
             "e2e": {"value": e2e_paths / (e2e_ms / 1e3), "unit": UNIT, "steps": ke, "ms_per_step": e2e_ms / ke,
                     "h2d_bytes_per_step": int(tris_h.numel() * 4 + att_h.numel()),
@@ -816,6 +818,42 @@ def cpu_baseline(R, seconds=15.0):
                      f"= {int(st[0])} path solves in {dt:.1f} s"}
     out["stages"] = cpu_stages(R, lib, kind, solve_paths_per_s=paths_per_s)
     return out
+
+
+def fp64_error(R, n=100000):
+    """Error of the headline image against FP64 on a sample of the frame's work items: the
+    batched solve (the headline's settings) of the sample alone on the GPU, against the
+    oracle's FP64 instantiation of the same per-path functions on the same inputs (and the
+    oracle's FP32 instantiation, which equals the reference's float arithmetic, beside it)."""
+    import torch
+    import oracle as O
+    A, sc = R.A, R.sc
+    m = R.n_paths
+    pairs = R.frame.paths[: m * 8].cpu().numpy().view(np.int32).reshape(-1, 2)
+    sel = _sample(pairs, n, 3)
+    cache = R.cache.to_host()
+    fd = R.frame.fd.cpu().numpy().view(np.float32).reshape(-1, 10)
+    nodes = np.frombuffer(R.ds.internals[: (R.ds.n - 1) * 64].cpu().numpy().tobytes(), O.NODE_DTYPE)
+    bvh = {"nodes": nodes, "root": R.ds.builder.root}
+    paths = torch.from_numpy(np.ascontiguousarray(sel).reshape(-1)).cuda()
+    spectral = torch.zeros_like(R.spectral)
+    d = A.solve_desc(R.ds, R.frame, R.cache, sc.events, len(sel), spectral=spectral, etas=R.etas,
+                     iteration=R.iteration, polish_det=POLISH_DET, fold_det=R.fold_det)
+    d.paths = paths.data_ptr()
+    A.solve_specular_batched(d, A.Scratch())
+    torch.cuda.synchronize()
+    gpu = spectral.cpu().numpy().astype(np.float64)
+    orc = O.oracle()
+    etas = sc.bin_etas()
+    img64, _ = orc.render_pairs(2, sel, cache, fd, bvh, sc, etas, dtype=np.float64, iteration=R.iteration)
+    img32, _ = orc.render_pairs(2, sel, cache, fd, bvh, sc, etas, dtype=np.float32, iteration=R.iteration)
+
+    def rel(a, b):
+        b = b.astype(np.float64)
+        return float(np.sqrt(((a.astype(np.float64) - b) ** 2).mean() / max((b ** 2).mean(), 1e-300)))
+    return {"batched_vs_fp64": rel(gpu, img64), "oracle_fp32_vs_fp64": rel(img32, img64),
+            "batched_vs_oracle_fp32": rel(gpu, img32),
+            "sample": f"{len(sel)} of the frame's {m} work items x {sc.n_bins} bins, spectral image rel. RMSE"}
 
 
 def cpu_stages(R, lib, kind, solve_paths_per_s, reps=5):

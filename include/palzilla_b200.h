@@ -275,9 +275,11 @@ PZ_API size_t pz_solve_batched_scratch_bytes(int K, uint64_t max_paths);
 /* After a batched solve: the scratch header holds u64 diagnostics at byte offset 64:
  * items skipped by prediction, predicted, plain fallback, per-bin Newton solves, FP64
  * polishes, visibility-query overflows, visibility candidates, visibility queries,
- * fallbacks because the centre solve did not converge, fallbacks because the predicted
- * shift over the band was too large, fallbacks because a probe disagreed with the predicted
- * branch, phase-2 Newton iterations, phase-2 bins refined from a predicted root. */
+ * fallbacks because the centre solve did not converge, fallbacks of items whose branch
+ * converged (near a fold, or a predicted shift over the band too large), fallbacks because a
+ * probe disagreed with the predicted branch, phase-2 Newton iterations, phase-2 bins refined
+ * from a predicted root, fallbacks near a fold (relative det below fold_det; part of the
+ * converged-branch fallbacks). */
 PZ_API int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32_t* n_paths_dev, void* scratch_dev,
                                      size_t scratch_bytes, int blocks_per_sm, pz_stream_t stream);
 

@@ -333,7 +333,7 @@ def solve_specular_batched(desc, scratch: Scratch, n_paths_dev=None, blocks_per_
 
 BATCH_COUNTERS = ("skipped", "predicted", "fallback", "newton_bins", "fp64_polish", "vis_overflow", "vis_candidates",
                   "vis_queries", "fallback_noconv", "fallback_shift", "fallback_probe", "newton_iterations",
-                  "newton_bins_refined")
+                  "newton_bins_refined", "fallback_fold")
 
 
 def batched_counters(scratch: Scratch) -> dict:

@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
     auto* recs = reinterpret_cast<PairRec<K>*>(a.records);
     unsigned long long nItems = 0;
     // diagnostic counts, kept per thread and added once at the end
-    unsigned long long cMode0 = 0, cMode1 = 0, cMode2 = 0, cProbe = 0, cShift = 0, cNoConv = 0;
+    unsigned long long cMode0 = 0, cMode1 = 0, cMode2 = 0, cProbe = 0, cShift = 0, cNoConv = 0, cFold = 0;
     for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < nPaths;
          idx += (uint64_t)gridDim.x * blockDim.x) {
         const SceneRef R = item_scene<kMulti>(a, idx);
@@ -555,6 +555,7 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
             if (minDet < a.illDet) {
                 // near a fold of the root curve: plain per-bin solves, FP64 polish when near-singular
                 r.polish = (double)minDet < a.polishDet ? 1 : 0;
+                cFold++;
             } else if (ca && cb && finite && nonlin < kMaxShift) {
                 // A bin contributes only if its root lies inside every triangle, so a bin whose
                 // predicted root is outside by more than the prediction error cannot contribute.
@@ -616,18 +617,28 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
             cShift += conv && conv2;
             cNoConv += !(conv && conv2);
         }
-        // warp-aggregated append of the items that have work
-        const bool keep = r.mode != 0;
+        // warp-aggregated appends of the items that have work: predicted items from the front
+        // of the records array, items solved bin by bin from its end
+        const bool keep1 = r.mode == 1, keep2 = r.mode == 2;
         const uint32_t active = __activemask();
-        const uint32_t ballot = __ballot_sync(active, keep);
+        const uint32_t lt = (1u << (threadIdx.x & 31)) - 1u;
+        const uint32_t b1 = __ballot_sync(active, keep1), b2 = __ballot_sync(active, keep2);
         const int leader = __ffs(active) - 1;
-        unsigned long long slot0 = 0;
-        if ((int)(threadIdx.x & 31) == leader && ballot)
-            slot0 = atomicAdd(a.recordCount, (unsigned long long)__popc(ballot));
-        slot0 = __shfl_sync(active, slot0, leader);
-        if (keep) {
-            const unsigned long long dst = slot0 + __popc(ballot & ((1u << (threadIdx.x & 31)) - 1u));
+        unsigned long long s1 = 0, s2 = 0;
+        if ((int)(threadIdx.x & 31) == leader) {
+            if (b1) s1 = atomicAdd(a.recordCount, (unsigned long long)__popc(b1));
+            if (b2) s2 = atomicAdd(a.recordCount2, (unsigned long long)__popc(b2));
+        }
+        s1 = __shfl_sync(active, s1, leader);
+        s2 = __shfl_sync(active, s2, leader);
+        if (keep1) {
+            const unsigned long long dst = s1 + __popc(b1 & lt);
             if (dst < a.recordCapacity) recs[dst] = r;
+            else raise_error(a.status, kErrCapacity);
+        }
+        if (keep2) {
+            const unsigned long long k = s2 + __popc(b2 & lt);
+            if (k < a.recordCapacity) recs[a.recordCapacity - 1 - k] = r;
             else raise_error(a.status, kErrCapacity);
         }
     }
@@ -639,6 +650,7 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
         flush_count(a.counters + kCntFallbackProbe, cProbe);
         flush_count(a.counters + kCntFallbackShift, cShift);
         flush_count(a.counters + kCntFallbackNoConv, cNoConv);
+        flush_count(a.counters + kCntFallbackFold, cFold);
     }
 }
 
@@ -678,13 +690,25 @@ PZ_D unsigned long long record_todo(const PairRec<K>& r, int B)
     return r.mode == 2 ? (B == 64 ? ~0ull : ((1ull << B) - 1ull)) : r.mask;
 }
 
+// m without its n lowest set bits.
+PZ_D unsigned long long drop_low_bits(unsigned long long m, int n)
+{
+    if (n >= __popcll(m)) return 0ull;
+    const int p = nth_bit64(m, n);
+    return m & ~((1ull << p) - 1ull);
+}
+
 template <int K, bool kMulti>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_p2_solve(BatchArgs a)
 {
     const int lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
     const int B = a.s.nBins;
-    const unsigned long long nRec = min(*a.recordCount, a.recordCapacity);
+    // The records solved bin by bin (the second queue) come first, then the predicted ones:
+    // one index space [0, nRec2 + nRec1) on one work counter, so a wave stops taking records
+    // only when its accepted list is full or every record is taken.
+    const unsigned long long nRec2 = min(*a.recordCount2, a.recordCapacity);
+    const unsigned long long nRec = nRec2 + min(*a.recordCount, a.recordCapacity);
     const auto* recs = reinterpret_cast<const PairRec<K>*>(a.records);
     auto* acc = reinterpret_cast<Accepted<K>*>(a.accepted);
     auto* blocks = reinterpret_cast<AcceptBlock*>(a.blocks);
@@ -692,101 +716,133 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_p2_solve(BatchArgs a
     unsigned long long* const nBlocks = a.p2 + 1;
     unsigned long long* const reserved = a.p2 + 2;
     unsigned long long nConv = 0, cNewton = 0, cPolish = 0, cIters = 0, cWarm = 0;
+    // The warp's current record and the bins of it not yet handed to a lane (warp-uniform).
+    unsigned long long jc = 0, mc = 0;
+    bool drained = false;
     for (;;) {
-        // one record per queue access, after reserving room for its accepted roots in this wave
-        unsigned long long j = 0;
-        bool take = false;
-        if (lane == 0) {
-            if (*a.workCounter < nRec && atomicAdd(reserved, 64ull) + 64ull <= a.acceptCapacity) {
-                j = atomicAdd(a.workCounter, 1ull);
-                take = j < nRec;
-            }
-        }
-        take = __shfl_sync(0xFFFFFFFFu, take, 0);
-        if (!take) break;
-        j = __shfl_sync(0xFFFFFFFFu, j, 0);
-        const PairRec<K> r = recs[j];
-        const SolveArgs& S = kMulti ? a.scenes[r.scene].s : a.s;
-        const float eta_c = S.etas[B / 2];
-        const V3<float> L = v3f<float>(S.p_light);
-        const int4 ti = S.cache.tris[r.slot];
-        const int tix[4] = {ti.x, ti.y, ti.z, ti.w};
-        Chain<K> ch;
-        load_chain<K>(ch, S.tris, S.attribs, tix);
-        const float3 pe = S.fds[r.pixel].p;
-        const V3<float> p = v3f<float>(pe);
-        float x0[2 * K];
-        {
-            const float4 q0 = S.cache.params[2 * r.slot], q1 = S.cache.params[2 * r.slot + 1];
-            const float pp[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-#pragma unroll
-            for (int i = 0; i < 2 * K; i++) x0[i] = pp[i];
-        }
-        const unsigned long long todo = record_todo<K>(r, B);
-        const int nTodo = __popcll(todo);
-        for (int round = 0; round * 32 < nTodo; round++) {
-            const int rank = lane + 32 * round;
-            const int b = rank < nTodo ? nth_bit64(todo, rank) : B;
-            float xs[2 * K];
-            float thr = 0.0f;
-            if (b < B) {
-                const float eta = S.etas[b];
-                const bool warm = r.mode == 1 && (a.continuation || ((r.warm >> b) & 1ull));
-                if (warm) {
-                    predict_root<K>(xs, r, eta, S.etas[0], eta_c, S.etas[B - 1]);
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 2 * K; i++) xs[i] = x0[i];
-                }
-                float det = 1.0f;
-                int its = 0;
-                // a predicted root is refined by Newton; every other bin runs the plain path's
-                // solver from the photon's start, so its accept / reject decision is the plain one
-                const bool conv = newton_nl<K>(xs, ch, S.p_light, pe, eta, S.events, S.maxIterations,
-                                               S.costTolerance, S.earlyTermWarmUp, true, warm ? 1 : 0, &det, &its);
-                cNewton++;
-                cIters += its;
-                cWarm += warm;
-                if (conv && S.roots) {
-                    float* rt = S.roots + ((size_t)r.item * B + b) * 8;
-#pragma unroll
-                    for (int i = 0; i < 2 * K; i++) rt[i] = xs[i];
-                }
-                if (conv) {
-                    nConv++;
-                    const bool polish = r.polish || (double)det < a.polishDet ||
-                                        (a.grazeCos > 0.0f && min_abs_cos<K>(ch, xs, S.p_light, pe) < a.grazeCos);
-                    cPolish += polish;
-                    float3 vtx[K + 2], nrm[K + 2];
-                    if (polish)
-                        thr = polish_fp64<K>(xs, ch, S.p_light, pe, S.events, eta, vtx, nrm);
-                    else
-                        thr = pre_throughput<float, K>(xs, L, p, ch, S.events, eta, vtx, nrm);
-                }
-            }
-            // this round's accepted roots: one block of consecutive entries
-            const uint32_t ok = __ballot_sync(0xFFFFFFFFu, thr > 0.0f);
-            if (ok) {
-                unsigned long long first = 0;
+        // Fill the 32 lanes with (record, bin) pairs.  A record solved bin by bin (every bin
+        // from the photon's start) starts a round, or joins one only if all its bins fit, so
+        // the bins of a round mostly share one chain and one start and follow similar Newton
+        // paths.  A predicted record is packed: its bins in rank order, then the next
+        // record's, so no lane idles for a bin that a record's mask excludes.  A record is
+        // taken after reserving room for 64 accepted roots (a record never has more) in this
+        // wave.
+        int filled = 0;
+        unsigned long long myRec = 0;
+        int myBin = -1;
+        while (filled < 32) {
+            if (mc == 0) {
+                if (drained) break;
+                unsigned long long j = 0;
+                bool take = false;
                 if (lane == 0) {
-                    first = atomicAdd(nAccepted, (unsigned long long)__popc(ok));
-                    const unsigned long long bi = atomicAdd(nBlocks, 1ull);
-                    if (bi < a.blockCapacity && first + __popc(ok) <= a.acceptCapacity)
-                        blocks[bi] = AcceptBlock{(uint32_t)first, (uint32_t)j, (uint32_t)__popc(ok)};
-                    else
-                        raise_error(a.status, kErrCapacity);  // cannot happen: room was reserved
+                    if (*a.workCounter < nRec && atomicAdd(reserved, 64ull) + 64ull <= a.acceptCapacity) {
+                        j = atomicAdd(a.workCounter, 1ull);
+                        take = j < nRec;
+                    }
                 }
-                first = __shfl_sync(0xFFFFFFFFu, first, 0);
-                const unsigned long long dst = first + __popc(ok & lt);
-                if (thr > 0.0f && dst < a.acceptCapacity) {
-                    Accepted<K> e;
-                    e.rec = (uint32_t)j;
-                    e.bin = (uint32_t)b;
-                    e.thr = thr;
+                take = __shfl_sync(0xFFFFFFFFu, take, 0);
+                if (!take) {
+                    drained = true;
+                    break;
+                }
+                j = __shfl_sync(0xFFFFFFFFu, j, 0);
+                const bool whole = j < nRec2;
+                jc = whole ? a.recordCapacity - 1 - j : j - nRec2;
+                mc = record_todo<K>(recs[jc], B);
+                if (whole && filled != 0 && B > 32 - filled) break;  // it starts the next round
+                continue;
+            }
+            const int n = min(__popcll(mc), 32 - filled);
+            if (lane >= filled && lane < filled + n) {
+                myRec = jc;
+                myBin = nth_bit64(mc, lane - filled);
+            }
+            mc = drop_low_bits(mc, n);
+            filled += n;
+        }
+        if (filled == 0) break;
+        float xs[2 * K];
+        float thr = 0.0f;
+        if (myBin >= 0) {
+            const int b = myBin;
+            const PairRec<K> r = recs[myRec];
+            const SolveArgs& S = kMulti ? a.scenes[r.scene].s : a.s;
+            const float eta_c = S.etas[B / 2];
+            const V3<float> L = v3f<float>(S.p_light);
+            const int4 ti = S.cache.tris[r.slot];
+            const int tix[4] = {ti.x, ti.y, ti.z, ti.w};
+            Chain<K> ch;
+            load_chain<K>(ch, S.tris, S.attribs, tix);
+            const float3 pe = S.fds[r.pixel].p;
+            const V3<float> p = v3f<float>(pe);
+            const float eta = S.etas[b];
+            const bool warm = r.mode == 1 && (a.continuation || ((r.warm >> b) & 1ull));
+            if (warm) {
+                predict_root<K>(xs, r, eta, S.etas[0], eta_c, S.etas[B - 1]);
+            } else {
+                const float4 q0 = S.cache.params[2 * r.slot], q1 = S.cache.params[2 * r.slot + 1];
+                const float pp[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
 #pragma unroll
-                    for (int i = 0; i < 2 * K; i++) e.x[i] = xs[i];
-                    acc[dst] = e;
-                }
+                for (int i = 0; i < 2 * K; i++) xs[i] = pp[i];
+            }
+            float det = 1.0f;
+            int its = 0;
+            // a predicted root is refined by Newton; every other bin runs the plain path's
+            // solver from the photon's start, so its accept / reject decision is the plain one
+            const bool conv = newton_nl<K>(xs, ch, S.p_light, pe, eta, S.events, S.maxIterations, S.costTolerance,
+                                           S.earlyTermWarmUp, true, warm ? 1 : 0, &det, &its);
+            cNewton++;
+            cIters += its;
+            cWarm += warm;
+            if (conv && S.roots) {
+                float* rt = S.roots + ((size_t)r.item * B + b) * 8;
+#pragma unroll
+                for (int i = 0; i < 2 * K; i++) rt[i] = xs[i];
+            }
+            if (conv) {
+                nConv++;
+                const bool polish = r.polish || (double)det < a.polishDet ||
+                                    (a.grazeCos > 0.0f && min_abs_cos<K>(ch, xs, S.p_light, pe) < a.grazeCos);
+                cPolish += polish;
+                float3 vtx[K + 2], nrm[K + 2];
+                if (polish)
+                    thr = polish_fp64<K>(xs, ch, S.p_light, pe, S.events, eta, vtx, nrm);
+                else
+                    thr = pre_throughput<float, K>(xs, L, p, ch, S.events, eta, vtx, nrm);
+            }
+        }
+        // This round's accepted roots: one block of consecutive entries per record.  A
+        // record's bins sit on consecutive lanes, so ordering the entries by lane keeps each
+        // record's entries together.
+        const uint32_t ok = __ballot_sync(0xFFFFFFFFu, thr > 0.0f);
+        if (ok) {
+            const uint32_t grp = __match_any_sync(0xFFFFFFFFu, myBin >= 0 ? myRec : ~0ull) & ok;
+            const bool leader = grp != 0 && lane == __ffs(grp) - 1;
+            const uint32_t leaders = __ballot_sync(0xFFFFFFFFu, leader);
+            unsigned long long first = 0, bi0 = 0;
+            if (lane == 0) {
+                first = atomicAdd(nAccepted, (unsigned long long)__popc(ok));
+                bi0 = atomicAdd(nBlocks, (unsigned long long)__popc(leaders));
+            }
+            first = __shfl_sync(0xFFFFFFFFu, first, 0);
+            bi0 = __shfl_sync(0xFFFFFFFFu, bi0, 0);
+            const unsigned long long dst = first + __popc(ok & lt);
+            if (leader) {
+                const unsigned long long bi = bi0 + __popc(leaders & lt);
+                if (bi < a.blockCapacity && dst + __popc(grp) <= a.acceptCapacity)
+                    blocks[bi] = AcceptBlock{(uint32_t)dst, (uint32_t)myRec, (uint32_t)__popc(grp)};
+                else
+                    raise_error(a.status, kErrCapacity);  // cannot happen: room was reserved
+            }
+            if (thr > 0.0f && dst < a.acceptCapacity) {
+                Accepted<K> e;
+                e.rec = (uint32_t)myRec;
+                e.bin = (uint32_t)myBin;
+                e.thr = thr;
+#pragma unroll
+                for (int i = 0; i < 2 * K; i++) e.x[i] = xs[i];
+                acc[dst] = e;
             }
         }
     }
@@ -802,10 +858,19 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_p2_solve(BatchArgs a
 template <int K, bool kMulti>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, 3) k_p2_vis(BatchArgs a)
 {
+    constexpr int NS = K + 1;
     __shared__ uint32_t cand[kWarpsPerBlock][kMaxCand];
     __shared__ uint32_t front[kWarpsPerBlock][2 * kFront];
+    // every root's shadow segments, so that any lane can test any (candidate, root) pair
+    __shared__ float3 segA[kWarpsPerBlock][NS][32], segD[kWarpsPerBlock][NS][32];
+    __shared__ uint32_t occMask[kWarpsPerBlock];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned long long nB = min(a.p2[1], a.blockCapacity);
+    // every record is taken by the last wave (each wave takes a fixed share or the rest); a
+    // record left over would be a missing contribution, so it is reported
+    if (a.wave == kMaxWaves - 1 && blockIdx.x == 0 && threadIdx.x == 0 &&
+        *a.workCounter < min(*a.recordCount, a.recordCapacity) + min(*a.recordCount2, a.recordCapacity))
+        raise_error(a.status, kErrCapacity);
     const auto* recs = reinterpret_cast<const PairRec<K>*>(a.records);
     auto* acc = reinterpret_cast<Accepted<K>*>(a.accepted);
     const auto* blocks = reinterpret_cast<const AcceptBlock*>(a.blocks);
@@ -835,7 +900,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 3) k_p2_vis(BatchArgs a)
         }
         // the shadow segments of every root: endpoints are the chain's vertices and shading
         // normals (contributableThroughput, pk.h:763-789), offset as occluded() does
-        constexpr int NS = K + 1;
         float3 sa[NS], sd[NS];
 #pragma unroll
         for (int sg = 0; sg < NS; sg++) sa[sg] = sd[sg] = mk3(0.f, 0.f, 0.f);
@@ -884,26 +948,58 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 3) k_p2_vis(BatchArgs a)
                 if (nc < 0) cOverflow++;
                 else cCand += (unsigned long long)nc;
             }
-            if (thr > 0.0f) {
+            if (nc < 0) {
+                // the candidate list overflowed: each root walks the BVH itself
                 bool occ = false;
-                if (nc < 0) {
+                if (thr > 0.0f) {
 #pragma unroll 1
                     for (int sg = 0; sg < NS && !occ; sg++)
                         occ = any_hit(S.nodes, S.tris, root, pick3<NS>(sa, sg), pick3<NS>(sd, sg), 1.0f) < 1.0f;
-                } else {
-                    for (int c = 0; c < nc && !occ; c++) {
+                }
+                if (occ) thr = 0.0f;
+            } else if (nc > 0) {
+                // The nc x nv (candidate, root) tests are spread over all 32 lanes, candidate
+                // major (neighbouring lanes load the same triangle), instead of each root's lane
+                // testing every candidate while the lanes without a root idle.  A root is
+                // occluded when any of its tests hits before the segment's end; tests of roots
+                // already found occluded are skipped.
+                if (thr > 0.0f) {
+#pragma unroll
+                    for (int sg = 0; sg < NS; sg++) {
+                        segA[warp][sg][lane] = sa[sg];
+                        segD[warp][sg][lane] = sd[sg];
+                    }
+                }
+                if (lane == 0) occMask[warp] = 0u;
+                __syncwarp();
+                const int nv = __popc(valid);
+                const int total = nc * nv;
+                const int dq = 32 / nv, dr = 32 % nv;
+                int c = lane / nv, rr = lane % nv;
+                volatile uint32_t* occ = &occMask[warp];
+                for (int pIdx = lane; pIdx < total; pIdx += 32) {
+                    const int src = (int)__fns(valid, 0, rr + 1);
+                    if (!((*occ >> src) & 1u)) {
                         const uint32_t e = cand[warp][c];
                         const uint32_t sg = e >> kSegShift;
                         float3 v0, v1, v2;
                         load_tri(S.tris, e & kIdxMask, v0, v1, v2);
                         float t, u, v;
                         float3 ng;
-                        if (ray_triangle(&t, &u, &v, &ng, 0.0f, 1.0f, pick3<NS>(sa, sg), pick3<NS>(sd, sg), v0, v1, v2) &&
+                        if (ray_triangle(&t, &u, &v, &ng, 0.0f, 1.0f, segA[warp][sg][src], segD[warp][sg][src], v0, v1,
+                                         v2) &&
                             t < 1.0f)
-                            occ = true;
+                            atomicOr(&occMask[warp], 1u << src);
+                    }
+                    c += dq;
+                    rr += dr;
+                    if (rr >= nv) {
+                        rr -= nv;
+                        c++;
                     }
                 }
-                if (occ) thr = 0.0f;
+                __syncwarp();
+                if ((occMask[warp] >> lane) & 1u) thr = 0.0f;
             }
             __syncwarp();
         }
@@ -957,9 +1053,11 @@ static cudaError_t launch_phases(const BatchArgs& a, int blocksPerSM, int p1Bloc
     for (int w = 0; w < kMaxWaves; w++) {
         cudaError_t e = cudaMemsetAsync(a.p2, 0, 4 * sizeof(unsigned long long), s);
         if (e != cudaSuccess) return e;
-        k_p2_solve<K, kMulti><<<sms * blocksPerSM, kWarpsPerBlock * 32, 0, s>>>(a);
-        k_p2_vis<K, kMulti><<<sms * 3, kWarpsPerBlock * 32, 0, s>>>(a);
-        k_p2_contrib<K, kMulti><<<sms * 8, 256, 0, s>>>(a);
+        BatchArgs aw = a;
+        aw.wave = w;
+        k_p2_solve<K, kMulti><<<sms * blocksPerSM, kWarpsPerBlock * 32, 0, s>>>(aw);
+        k_p2_vis<K, kMulti><<<sms * 3, kWarpsPerBlock * 32, 0, s>>>(aw);
+        k_p2_contrib<K, kMulti><<<sms * 8, 256, 0, s>>>(aw);
     }
     return cudaGetLastError();
 }
@@ -1009,8 +1107,8 @@ size_t record_bytes(int K)
 cudaError_t launch_solve_batched(int K, const BatchArgs& a, int blocksPerSM, cudaStream_t s)
 {
     if (a.s.nBins < 1 || a.s.nBins > 64) return cudaErrorInvalidValue;
-    cudaError_t e = cudaMemsetAsync(a.workCounter, 0, sizeof(unsigned long long), s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(a.recordCount, 0, sizeof(unsigned long long), s);
+    // work counter, record count and the second queue's two words are consecutive header words
+    cudaError_t e = cudaMemsetAsync(a.workCounter, 0, 4 * sizeof(unsigned long long), s);
     if (e != cudaSuccess) return e;
     switch (K) {
         case 1: return launch_k<1>(a, blocksPerSM, s);
@@ -1025,8 +1123,8 @@ cudaError_t launch_solve_batched_multi(int K, const BatchArgs& a, int p1BlocksPe
                                        unsigned long long* offsets, cudaStream_t s)
 {
     if (a.s.nBins < 1 || a.s.nBins > 64 || !a.scenes || a.nScenes == 0) return cudaErrorInvalidValue;
-    cudaError_t e = cudaMemsetAsync(a.workCounter, 0, sizeof(unsigned long long), s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(a.recordCount, 0, sizeof(unsigned long long), s);
+    // work counter, record count and the second queue's two words are consecutive header words
+    cudaError_t e = cudaMemsetAsync(a.workCounter, 0, 4 * sizeof(unsigned long long), s);
     if (e != cudaSuccess) return e;
     k_scene_offsets<<<1, 1024, 0, s>>>(a.scenes, a.nScenes, offsets);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -12,6 +12,11 @@ struct BatchArgs {
     const uint32_t* nPathsDev;         // device item count (the lookup counter), or null: s.nPaths
     unsigned long long* workCounter;   // device scratch word (zeroed by the launcher)
     unsigned long long* recordCount;   // device scratch word (zeroed by the launcher)
+    // Records of items solved bin by bin (every bin from the photon's start) form a second
+    // queue, filled from the end of the records array; each item makes at most one record and
+    // the capacity covers every item, so the two queues never meet.
+    unsigned long long* workCounter2;  // device scratch word (zeroed by the launcher)
+    unsigned long long* recordCount2;  // device scratch word (zeroed by the launcher)
     void* records;                     // phase-1 records, recordCapacity of record_bytes(K)
     unsigned long long recordCapacity;
     void* probes;                      // plain-solve probes, 3 per work item of probe_bytes(K), s.nPaths items
@@ -32,19 +37,24 @@ struct BatchArgs {
     unsigned long long blockCapacity = 0;
     unsigned long long* p2 = nullptr;  // device u64[4] (scratch header byte 192): accepted count, block count,
                                        // reserved, blocks taken
+    int wave = 0;                      // phase-2 wave of this launch (0 .. kMaxWaves - 1)
 };
 
 // Phase 2 runs in at most kMaxWaves waves; each wave has room for 64 accepted roots (a record's
 // most) per record of 1/kMaxWaves of the record capacity, so every record fits.
 constexpr int kMaxWaves = 8;
+// Relative determinant of an item's branch of roots below which the item is solved bin by bin
+// (near a fold of the caustic, where the prediction of the bins' roots is least reliable).
+constexpr float kDefaultFoldDet = 1.0e-2f;
 inline unsigned long long accept_capacity(unsigned long long recordCapacity)
 {
     return 64ull * ((recordCapacity + kMaxWaves - 1) / kMaxWaves);
 }
-// at most two rounds (blocks) per record: B <= 64 bins, 32 lanes
+// at most three rounds (blocks) per record: B <= 64 bins on consecutive lanes of 32-lane
+// rounds that other records' bins may start and end
 inline unsigned long long block_capacity(unsigned long long recordCapacity)
 {
-    return 2ull * ((recordCapacity + kMaxWaves - 1) / kMaxWaves);
+    return 3ull * ((recordCapacity + kMaxWaves - 1) / kMaxWaves);
 }
 
 // One scene of a batch: its solve arguments and its item count on the device.
@@ -56,7 +66,7 @@ struct SceneArgs {
 // diagnostics counters
 enum {
     kCntMode0 = 0, kCntMode1, kCntMode2, kCntNewton2, kCntPolish, kCntFatOverflow, kCntCandidates, kCntQueries,
-    kCntFallbackNoConv, kCntFallbackShift, kCntFallbackProbe, kCntNewtonIters, kCntWarm, kNumCounters
+    kCntFallbackNoConv, kCntFallbackShift, kCntFallbackProbe, kCntNewtonIters, kCntWarm, kCntFallbackFold, kNumCounters
 };
 
 // bytes of one phase-1 record for chain length K

@@ -275,6 +275,8 @@ extern "C" int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32
     b.status = reinterpret_cast<uint32_t*>(base);
     b.workCounter = reinterpret_cast<unsigned long long*>(base + 8);
     b.recordCount = reinterpret_cast<unsigned long long*>(base + 16);
+    b.workCounter2 = reinterpret_cast<unsigned long long*>(base + 24);
+    b.recordCount2 = reinterpret_cast<unsigned long long*>(base + 32);
     const BatchLayout L = batch_layout(desc->K, desc->n_paths, 256);
     b.records = base + L.records;
     b.recordCapacity = desc->n_paths;
@@ -290,7 +292,7 @@ extern "C" int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32
     b.polishDet = desc->polish_det > 0.0f ? (double)desc->polish_det : 0.0;
     b.grazeCos = desc->graze_cos > 0.0f ? desc->graze_cos : 0.0f;
     b.continuation = desc->continuation;
-    b.illDet = desc->fold_det < 0.0f ? 0.0f : (desc->fold_det == 0.0f ? 1.0e-2f : desc->fold_det);
+    b.illDet = desc->fold_det < 0.0f ? 0.0f : (desc->fold_det == 0.0f ? batched::kDefaultFoldDet : desc->fold_det);
     if (desc->n_paths == 0) { clear_error(); return PZ_OK; }
     cudaError_t e = cudaMemsetAsync(base, 0, 256, S(stream));
     if (e == cudaSuccess) e = batched::launch_solve_batched(desc->K, b, blocks_per_sm > 0 ? blocks_per_sm : 2, S(stream));
@@ -401,6 +403,8 @@ static int multi_args(int K, int n_bins, uint32_t n_scenes, uint64_t total, void
     b->status = reinterpret_cast<uint32_t*>(base);
     b->workCounter = reinterpret_cast<unsigned long long*>(base + 8);
     b->recordCount = reinterpret_cast<unsigned long long*>(base + 16);
+    b->workCounter2 = reinterpret_cast<unsigned long long*>(base + 24);
+    b->recordCount2 = reinterpret_cast<unsigned long long*>(base + 32);
     b->counters = reinterpret_cast<unsigned long long*>(base + 64);
     b->records = base + L.records;
     b->recordCapacity = total;
@@ -413,7 +417,7 @@ static int multi_args(int K, int n_bins, uint32_t n_scenes, uint64_t total, void
     b->polishDet = 0.0;
     b->grazeCos = 0.0f;
     b->continuation = 0;
-    b->illDet = 1.0e-2f;
+    b->illDet = batched::kDefaultFoldDet;
     b->scenes = reinterpret_cast<const batched::SceneArgs*>(base + L.table);
     b->nScenes = n_scenes;
     *offsets = reinterpret_cast<unsigned long long*>(base + L.offsets);

@@ -19,7 +19,11 @@ namespace pz {
 
 constexpr int kPhotonDepth = 4;  // PHOTON_TRACE_MAX_DEPTH, pk.h:33
 
-__global__ void __launch_bounds__(256) k_photon(const Node* __restrict__ nodes, const uint32_t* __restrict__ rootPtr,
+#ifndef PZ_PHOTON_MIN_BLOCKS
+#define PZ_PHOTON_MIN_BLOCKS 1
+#endif
+
+__global__ void __launch_bounds__(256, PZ_PHOTON_MIN_BLOCKS) k_photon(const Node* __restrict__ nodes, const uint32_t* __restrict__ rootPtr,
                                                 const Tri* __restrict__ tris, const Attrib* __restrict__ attribs,
                                                 uint32_t nTris, uint32_t photonsPerTri, float3 p_light, float eta_min,
                                                 float eta_max, int iteration, float minThroughput, CacheView cache,

@@ -50,6 +50,25 @@ def batch():
     return items, ref
 
 
+def test_single_scene_solves_repeat(batch):
+    """Each scene's batched solve, run again on fresh scratch, gives the same image (up to the
+    order of the float atomics) and a clean status word.  The batch holds scenes whose items
+    are nearly all solved bin by bin (so their records fill every phase-2 wave) and scenes
+    that are mostly predicted."""
+    items, ref = batch
+    modes = []
+    for i, it in enumerate(items):
+        it.spectral.zero_()
+        scratch = A.Scratch()
+        A.solve_specular_batched(it.desc(), scratch)
+        torch.cuda.synchronize()
+        assert _rel(it.spectral, ref[i]) <= 1e-6, i
+        assert scratch.status() == 0, i
+        c = A.batched_counters(scratch)
+        modes.append(c["fallback"] / max(1, c["skipped"] + c["predicted"] + c["fallback"]))
+    assert max(modes) > 0.9 and min(modes) < 0.1, modes
+
+
 @pytest.mark.parametrize("K", [1, 2])
 @pytest.mark.parametrize("device_counts", [False, True])
 def test_batch_matches_single_scene_solves(batch, K, device_counts):
