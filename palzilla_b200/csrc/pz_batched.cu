@@ -719,6 +719,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_p2_solve(BatchArgs a
     // The warp's current record and the bins of it not yet handed to a lane (warp-uniform).
     unsigned long long jc = 0, mc = 0;
     bool drained = false;
+    // accepted roots held back for the next round: ns entries of record stashRec
+    __shared__ Accepted<K> stash[kWarpsPerBlock][32];
+    const int warp = threadIdx.x >> 5;
+    int ns = 0;
+    unsigned long long stashRec = 0;
     for (;;) {
         // Fill the 32 lanes with (record, bin) pairs.  A record solved bin by bin (every bin
         // from the photon's start) starts a round, or joins one only if all its bins fit, so
@@ -812,39 +817,76 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_p2_solve(BatchArgs a
                     thr = pre_throughput<float, K>(xs, L, p, ch, S.events, eta, vtx, nrm);
             }
         }
-        // This round's accepted roots: one block of consecutive entries per record.  A
+        // This round's accepted roots, as blocks of consecutive entries, one per record: a
         // record's bins sit on consecutive lanes, so ordering the entries by lane keeps each
-        // record's entries together.
+        // record's entries together.  The roots of a record that continues into the next round
+        // are held in the warp's stash and leave with that record's next roots, so a record
+        // split between rounds still makes one block (one shared visibility query) when its
+        // roots number 32 or fewer.
         const uint32_t ok = __ballot_sync(0xFFFFFFFFu, thr > 0.0f);
-        if (ok) {
-            const uint32_t grp = __match_any_sync(0xFFFFFFFFu, myBin >= 0 ? myRec : ~0ull) & ok;
-            const bool leader = grp != 0 && lane == __ffs(grp) - 1;
-            const uint32_t leaders = __ballot_sync(0xFFFFFFFFu, leader);
+        const bool hasBin = myBin >= 0;
+        const uint32_t contMask = mc != 0 ? __ballot_sync(0xFFFFFFFFu, hasBin && myRec == jc) : 0u;
+        const uint32_t g0Mask = ns > 0 ? __ballot_sync(0xFFFFFFFFu, hasBin && myRec == stashRec) : 0u;
+        const uint32_t okS = ok & contMask, okE = ok & ~contMask;
+        const uint32_t g0E = okE & g0Mask;
+        bool emitStash = false, merged = false;
+        int keep = 0;
+        if (ns > 0) {
+            if ((g0Mask & contMask) != 0) {
+                // the stashed record continues once more
+                if (ns + __popc(okS) > 32) emitStash = true;
+                else keep = ns;
+            } else {
+                emitStash = true;
+                merged = ns + __popc(g0E) <= 32;
+            }
+        }
+        Accepted<K> e;
+        e.rec = (uint32_t)myRec;
+        e.bin = (uint32_t)myBin;
+        e.thr = thr;
+#pragma unroll
+        for (int i = 0; i < 2 * K; i++) e.x[i] = xs[i];
+        const int sOut = emitStash ? ns : 0;
+        const uint32_t grp = __match_any_sync(0xFFFFFFFFu, hasBin ? myRec : ~0ull) & okE;
+        const bool leader = grp != 0 && lane == __ffs(grp) - 1 && !(merged && ((g0Mask >> lane) & 1u));
+        const uint32_t leaders = __ballot_sync(0xFFFFFFFFu, leader);
+        const int nOut = sOut + __popc(okE);
+        if (nOut > 0) {
             unsigned long long first = 0, bi0 = 0;
             if (lane == 0) {
-                first = atomicAdd(nAccepted, (unsigned long long)__popc(ok));
-                bi0 = atomicAdd(nBlocks, (unsigned long long)__popc(leaders));
+                first = atomicAdd(nAccepted, (unsigned long long)nOut);
+                bi0 = atomicAdd(nBlocks, (unsigned long long)((emitStash ? 1 : 0) + __popc(leaders)));
             }
             first = __shfl_sync(0xFFFFFFFFu, first, 0);
             bi0 = __shfl_sync(0xFFFFFFFFu, bi0, 0);
-            const unsigned long long dst = first + __popc(ok & lt);
-            if (leader) {
-                const unsigned long long bi = bi0 + __popc(leaders & lt);
-                if (bi < a.blockCapacity && dst + __popc(grp) <= a.acceptCapacity)
-                    blocks[bi] = AcceptBlock{(uint32_t)dst, (uint32_t)myRec, (uint32_t)__popc(grp)};
+            // the stash's block: its entries, then (merged) the same record's roots of this round
+            if (emitStash && lane == 0) {
+                const uint32_t cnt = (uint32_t)(ns + (merged ? __popc(g0E) : 0));
+                if (bi0 < a.blockCapacity && first + cnt <= a.acceptCapacity)
+                    blocks[bi0] = AcceptBlock{(uint32_t)first, (uint32_t)stashRec, cnt};
                 else
                     raise_error(a.status, kErrCapacity);  // cannot happen: room was reserved
             }
-            if (thr > 0.0f && dst < a.acceptCapacity) {
-                Accepted<K> e;
-                e.rec = (uint32_t)myRec;
-                e.bin = (uint32_t)myBin;
-                e.thr = thr;
-#pragma unroll
-                for (int i = 0; i < 2 * K; i++) e.x[i] = xs[i];
-                acc[dst] = e;
+            if (leader) {
+                const unsigned long long bi = bi0 + (emitStash ? 1 : 0) + __popc(leaders & lt);
+                const unsigned long long dst = first + sOut + __popc(okE & lt);
+                if (bi < a.blockCapacity && dst + __popc(grp) <= a.acceptCapacity)
+                    blocks[bi] = AcceptBlock{(uint32_t)dst, (uint32_t)myRec, (uint32_t)__popc(grp)};
+                else
+                    raise_error(a.status, kErrCapacity);
+            }
+            if (emitStash && lane < ns && first + lane < a.acceptCapacity) acc[first + lane] = stash[warp][lane];
+            if ((okE >> lane) & 1u) {
+                const unsigned long long dst = first + sOut + __popc(okE & lt);
+                if (dst < a.acceptCapacity) acc[dst] = e;
             }
         }
+        __syncwarp();
+        if ((okS >> lane) & 1u) stash[warp][keep + __popc(okS & lt)] = e;
+        ns = contMask ? keep + __popc(okS) : 0;
+        stashRec = jc;
+        __syncwarp();
     }
     if (a.s.stats) flush_count(a.s.stats + 1, nConv);
     if (a.counters) {
@@ -862,7 +904,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 3) k_p2_vis(BatchArgs a)
     __shared__ uint32_t cand[kWarpsPerBlock][kMaxCand];
     __shared__ uint32_t front[kWarpsPerBlock][2 * kFront];
     // every root's shadow segments, so that any lane can test any (candidate, root) pair
-    __shared__ float3 segA[kWarpsPerBlock][NS][32], segD[kWarpsPerBlock][NS][32];
+    // (components apart, so that lanes reading different roots' segments hit different banks)
+    __shared__ float segA[kWarpsPerBlock][NS][3][32], segD[kWarpsPerBlock][NS][3][32];
     __shared__ uint32_t occMask[kWarpsPerBlock];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned long long nB = min(a.p2[1], a.blockCapacity);
@@ -966,8 +1009,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 3) k_p2_vis(BatchArgs a)
                 if (thr > 0.0f) {
 #pragma unroll
                     for (int sg = 0; sg < NS; sg++) {
-                        segA[warp][sg][lane] = sa[sg];
-                        segD[warp][sg][lane] = sd[sg];
+                        segA[warp][sg][0][lane] = sa[sg].x;
+                        segA[warp][sg][1][lane] = sa[sg].y;
+                        segA[warp][sg][2][lane] = sa[sg].z;
+                        segD[warp][sg][0][lane] = sd[sg].x;
+                        segD[warp][sg][1][lane] = sd[sg].y;
+                        segD[warp][sg][2][lane] = sd[sg].z;
                     }
                 }
                 if (lane == 0) occMask[warp] = 0u;
@@ -986,8 +1033,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 3) k_p2_vis(BatchArgs a)
                         load_tri(S.tris, e & kIdxMask, v0, v1, v2);
                         float t, u, v;
                         float3 ng;
-                        if (ray_triangle(&t, &u, &v, &ng, 0.0f, 1.0f, segA[warp][sg][src], segD[warp][sg][src], v0, v1,
-                                         v2) &&
+                        const float3 ro = mk3(segA[warp][sg][0][src], segA[warp][sg][1][src], segA[warp][sg][2][src]);
+                        const float3 rd = mk3(segD[warp][sg][0][src], segD[warp][sg][1][src], segD[warp][sg][2][src]);
+                        if (ray_triangle(&t, &u, &v, &ng, 0.0f, 1.0f, ro, rd, v0, v1, v2) &&
                             t < 1.0f)
                             atomicOr(&occMask[warp], 1u << src);
                     }
