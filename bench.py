@@ -51,10 +51,13 @@ POLISH_DET = 1.0e-6
 # k_reorder, k_probe, k_phase1, 8 phase-2 waves x (k_p2_solve, k_p2_vis, k_p2_contrib) (waves
 # without records exit at once), k_resolve_spectral
 LAUNCHES_PER_FRAME = 12 + 8 * 3
-# DRAM bytes (read + write) per work item of k_probe + k_phase1 + k_phase2, from one ncu
-# capture of the first frame of this workload (its light sample is the centre):
-# 6971.2 MB / 19.8 M items
-NCU_SOLVE_TRAFFIC_PER_ITEM = 352.1
+# Per work item of the batched solve stage (k_probe, k_phase1 and the 8 phase-2 waves of
+# k_p2_solve / k_p2_vis / k_p2_contrib), from one ncu capture of every launch of one frame
+# of this workload at 256x256 (1,256,661 work items; summarised under profiles/):
+# DRAM bytes read + written (1013.5 MB) and warp instructions issued (4.810 G).
+NCU_SOLVE_DRAM_PER_ITEM = 806.5
+NCU_SOLVE_WARP_INST_PER_ITEM = 3828.0
+ISSUE_PER_SM_PER_CLOCK = 4  # one warp instruction per cycle on each of an SM's 4 schedulers
 
 
 def peaks():
@@ -310,13 +313,25 @@ def run_ours(args):
     # + two triangles 72 + two attributes 80 = 248 B read once; 4 B per contributing (item, bin) added
     alg_bytes = n_items * 248.0 + contributing * 4.0
     achieved = alg_bytes / (solve_avg / 1e3) / 1e9
-    roofline = {"kernel": "k_probe + k_phase1 + k_phase2 (batched solve)", "bound": "hbm", "achieved": achieved,
-                "peak": hbm,
-                "unit": "GB/s", "frac": achieved / hbm, "peak_kind": hbm_kind,
-                "traffic": NCU_SOLVE_TRAFFIC_PER_ITEM * n_items if NCU_SOLVE_TRAFFIC_PER_ITEM else None,
-                "algorithmic_bytes": alg_bytes,
-                "note": "issue-bound (FP32 Newton/QR and BVH visibility in registers): the HBM fraction is "
-                        "small by design; SM issue and occupancy are in profiles/"}
+    # issue roofline of the same stage: warp instructions (per work item, from the capture)
+    # over the stage's time, against 4 schedulers x SMs x the SM clock sampled meanwhile
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    clk_mhz = clk.get("sm_mhz") or 1965.0
+    inst = NCU_SOLVE_WARP_INST_PER_ITEM * n_items
+    issue_achieved = inst / (solve_avg / 1e3) / 1e9
+    issue_peak = ISSUE_PER_SM_PER_CLOCK * sms * clk_mhz * 1e6 / 1e9
+    roofline = {"kernel": "batched solve stage: k_probe, k_phase1, 8 waves of k_p2_solve / k_p2_vis / k_p2_contrib",
+                "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "peak_kind": hbm_kind, "traffic": NCU_SOLVE_DRAM_PER_ITEM * n_items, "algorithmic_bytes": alg_bytes,
+                "traffic_note": "DRAM bytes per work item from an ncu capture of every launch of a 256x256 frame, "
+                                "scaled by this frame's work items",
+                "issue": {"bound": "issue", "achieved": issue_achieved, "peak": issue_peak,
+                          "unit": "G warp instructions/s", "frac": issue_achieved / issue_peak,
+                          "warp_instructions": inst,
+                          "note": "warp instructions per work item from the same capture; peak = 4 schedulers x "
+                                  f"{sms} SMs x the sampled SM clock"},
+                "note": "the stage is issue-bound (FP32 Newton/QR and BVH queries in registers, scene and BVH in "
+                        "L2): its HBM fraction is small by design, its issue fraction is the bound"}
 
     sort_build = bench_sort_build(hbm, hbm_kind) if (rank == 0 and not args.no_sort) else None
 
