@@ -586,6 +586,13 @@ struct SubArgs {
     uint64_t rootCapacity;
     unsigned long long* stats;
     uint32_t* status;
+    // box queue of the persistent subdivision kernel: a ring of ringCapacity entries and its
+    // claim / reserve / outstanding counters
+    uint64_t* ring;
+    uint64_t ringCapacity;
+    unsigned long long* qHead;     // entries claimed by consumers
+    unsigned long long* qTail;     // entries reserved by producers
+    unsigned long long* qPending;  // boxes pushed and not yet finished
 };
 
 // entry: row << 32 | depth << 20 | path
@@ -711,6 +718,276 @@ __global__ void __launch_bounds__(kBlock) k_sub_round(SubArgs a, int depth, cons
             }
         }
     }
+    if (a.stats) {
+        warp_sum(a.stats + kStTested, tested);
+        warp_sum(a.stats + kStCulled, culled);
+    }
+}
+
+// ---------------------------------------------------------------- persistent box queue
+// Tuples whose domains need very different depths share one persistent kernel fed by a
+// device-side queue (k_sub_queue below).  The queue is a ring of entries in the scratch's
+// two frontier regions: a slot holds an entry with kQueued set and the lap of its index, or
+// 0 when free.  A producer reserves indices on qTail and waits (bounded) until each slot is
+// free before storing; a consumer claims indices on qHead and takes a slot once its entry
+// (of the right lap) is stored, then frees it.  Every wait has an iteration limit (status
+// kErrSpinLimit); a ring too small for the live boxes sets kErrCapacity.  Which warp bounds
+// which box changes nothing: the leaves are a set (sorted by row afterwards), as with one
+// launch per depth.
+constexpr uint64_t kQueued = 1ull << 31;  // above the depth field of an entry
+constexpr int kLapShift = 25;              // bits 25-30: the ring lap of the entry's index
+constexpr uint64_t kLapMask = 63ull << kLapShift;
+constexpr uint32_t kQueueSpin = 1u << 22;
+static_assert(kMaxDepth + 5 <= kLapShift, "the lap bits sit above an entry's depth field");
+
+// an entry as stored in ring slot i % cap: queued bit and the lap i / cap (mod 64), so that a
+// consumer of index i never takes the entry of index i - cap still waiting in the slot
+PZ_D uint64_t queued_entry(uint64_t ent, uint64_t index, uint64_t cap)
+{
+    return ent | kQueued | (((index / cap) & 63ull) << kLapShift);
+}
+
+PZ_D unsigned long long ld_volatile(const unsigned long long* p)
+{
+    return *reinterpret_cast<const volatile unsigned long long*>(p);
+}
+
+// the first boxes: one per row at depth 0, and the queue counters
+__global__ void k_sub_queue_init(SubArgs a)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        float lo = 0.0f, hi = 0.0f;
+        for (uint32_t b = 0; b < a.nBins; b++) {
+            const float e = a.etas[b];
+            const float m = __fsub_rn(__fmul_rn(e, e), 1.0f);
+            lo = b == 0 ? m : fminf(lo, m);
+            hi = b == 0 ? m : fmaxf(hi, m);
+        }
+        a.em1[0] = lo;
+        a.em1[1] = hi;
+        *a.qHead = 0;
+        *a.qTail = a.nRows;
+        *a.qPending = a.nRows;
+    }
+    const uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row < a.nRows) a.ring[row] = queued_entry(make_entry(row, 0, 0u), row, a.ringCapacity);
+}
+
+constexpr int kLocal = 256;                 // entries of a warp's local box stack (shared memory)
+#ifndef PZ_SUBDIV_LEND_ABOVE
+#define PZ_SUBDIV_LEND_ABOVE 64
+#endif
+#ifndef PZ_SUBDIV_LEND_EVERY
+#define PZ_SUBDIV_LEND_EVERY 1
+#endif
+constexpr int kDonateAbove = PZ_SUBDIV_LEND_ABOVE;  // a warp holding more lends boxes to the ring when it runs low
+constexpr int kLendEvery = PZ_SUBDIV_LEND_EVERY;    // passes between two looks at the ring's level
+constexpr uint64_t kNoClaim = ~0ull;
+
+// Stores this lane's entry in the ring when `want`; all lanes of the warp call it.  False
+// when the ring is full (kErrCapacity) or a wait for a free slot gave up.
+PZ_D bool ring_push(const SubArgs& a, bool want, uint64_t ent)
+{
+    const unsigned long long i = warp_reserve(a.qTail, want ? 1u : 0u);
+    bool ok = true;
+    if (want) {
+        const uint64_t cap = a.ringCapacity;
+        volatile uint64_t* ring = a.ring;
+        if (i >= ld_volatile(a.qHead) + cap) {
+            // the slot's previous entry (index i - cap) is not even claimed: the ring is full
+            raise_error(a.status, kErrCapacity);
+            ok = false;
+        } else {
+            const uint64_t slot = i % cap;
+            uint32_t spin = 0;
+            while (ring[slot] != 0ull) {
+                if (++spin >= kQueueSpin) {
+                    ok = false;
+                    break;
+                }
+                __nanosleep(64);
+            }
+            if (ok) ring[slot] = queued_entry(ent, i, cap);
+        }
+    }
+    return __all_sync(0xFFFFFFFFu, ok);
+}
+
+// Persistent subdivision: each warp bounds up to 32 boxes per pass, taken from its own stack
+// of boxes in shared memory (newest first: depth first, so the stack stays short and a pass
+// mostly holds boxes of one tuple), else from the ring.  Children go to the warp's stack;
+// what does not fit goes to the ring, and a warp holding many boxes lends its oldest ones to
+// the ring whenever the ring runs low, so that idle warps share a deep tuple's boxes.
+// Claims on the ring are taken with one atomic add per warp; a claimed slot whose entry is
+// not stored yet is checked again on the next pass while the lane's other work goes on (no
+// lane waits on another warp's progress except for a free slot).  qPending counts the boxes
+// that exist anywhere; each warp keeps its own running change (children made minus boxes
+// bound) and adds it in before every push to the ring and whenever it runs out of work, so
+// the counter stays at or above the true count and reaches 0 only at the end.
+template <int K>
+__global__ void __launch_bounds__(kBlock) k_sub_queue(SubArgs a)
+{
+    constexpr int N = 2 * K;
+    __shared__ uint64_t stacks[kBlock / 32][kLocal];
+    const Af<N + 1> em1 = em1_form<N + 1>(a.em1[0], a.em1[1]);
+    const int lane = (int)(threadIdx.x & 31);
+    const uint32_t lt = (1u << lane) - 1u;
+    uint64_t* stk = stacks[threadIdx.x >> 5];
+    const uint64_t cap = a.ringCapacity;
+    volatile uint64_t* ring = a.ring;
+    const unsigned long long lowWater = (unsigned long long)gridDim.x * (kBlock / 32) * 32;
+    int top = 0;              // boxes on the warp's stack (warp-uniform)
+    long long delta = 0;      // boxes made minus boxes bound since the last add-in (warp-uniform)
+    uint64_t claim = kNoClaim;
+    uint32_t tested = 0, culled = 0, idle = 0, sleep = 64, passes = 0;
+    bool failed = false;
+    for (;;) {
+        uint64_t ent = 0;
+        bool have = false;
+        // (1) a claimed ring slot whose entry has been stored
+        if (claim != kNoClaim) {
+            const uint64_t slot = claim % cap;
+            const uint64_t v = ring[slot];
+            if ((v & (kQueued | kLapMask)) == queued_entry(0ull, claim, cap)) {
+                ring[slot] = 0ull;
+                ent = v & ~(kQueued | kLapMask);
+                have = true;
+                claim = kNoClaim;
+            }
+        }
+        // (2) free lanes take the newest boxes of the warp's stack
+        const uint32_t free1 = __ballot_sync(0xFFFFFFFFu, !have && claim == kNoClaim);
+        const int take = min(__popc(free1), top);
+        if ((free1 >> lane) & 1u) {
+            const int r = __popc(free1 & lt);
+            if (r < take) {
+                ent = stk[top - 1 - r];
+                have = true;
+            }
+        }
+        top -= take;
+        __syncwarp();
+        // (3) with the stack empty, lanes still free claim ring entries
+        const uint32_t free2 = __ballot_sync(0xFFFFFFFFu, !have && claim == kNoClaim);
+        if (top == 0 && free2) {
+            unsigned long long h = 0;
+            int c = 0;
+            if (lane == 0) {
+                const unsigned long long t = ld_volatile(a.qTail), h0 = ld_volatile(a.qHead);
+                if (h0 < t) {
+                    c = (int)min((unsigned long long)__popc(free2), t - h0);
+                    h = atomicAdd(a.qHead, (unsigned long long)c);
+                }
+            }
+            c = __shfl_sync(0xFFFFFFFFu, c, 0);
+            h = __shfl_sync(0xFFFFFFFFu, h, 0);
+            if ((free2 >> lane) & 1u) {
+                const int r = __popc(free2 & lt);
+                if (r < c) claim = h + (uint64_t)r;
+            }
+        }
+        const uint32_t work = __ballot_sync(0xFFFFFFFFu, have);
+        if (!work) {
+            if (top == 0) {
+                // out of work: add the running change in; stop once no box is left anywhere
+                // (then no entry will ever be stored in a slot still claimed here: such a
+                // claim ran ahead of the producers)
+                if (delta != 0) {
+                    if (lane == 0) atomicAdd(a.qPending, (unsigned long long)delta);
+                    delta = 0;
+                }
+                int done = 0;
+                if (lane == 0) done = ld_volatile(a.qPending) == 0 ? 1 : 0;
+                if (__shfl_sync(0xFFFFFFFFu, done, 0)) break;
+            }
+            if (++idle >= kQueueSpin) {
+                failed = true;
+                break;
+            }
+            __nanosleep(sleep);
+            sleep = min(sleep * 2, 2048u);
+            continue;
+        }
+        idle = 0;
+        sleep = 64;
+        // (4) bound the boxes
+        int v = kCull;
+        uint32_t row = 0, path = 0;
+        int depth = 0;
+        if (have) {
+            row = (uint32_t)(ent >> 32);
+            path = (uint32_t)ent & kPathMask;
+            depth = (int)(((uint32_t)ent >> kMaxDepth) & 31u);
+            Chain<K> ch;
+            uint32_t q;
+            load_row<K>(ch, a, row, &q);
+            float lo[N], hi[N];
+            box_bounds<N>(path, depth, lo, hi);
+            v = bound_box<K>(ch, a.pBeg, a.pEnd[q], a.events, em1, lo, hi, a.eps);
+            if (v == kSplit && depth >= a.maxDepth) v = kLeaf;
+            tested++;
+            culled += v == kCull;
+        }
+        const unsigned long long ls = warp_append(a.nLeaves, have && v == kLeaf);
+        if (have && v == kLeaf) {
+            if (ls < a.capacity) a.leaves[ls] = make_entry(row, depth, path);
+            else raise_error(a.status, kErrCapacity);
+        }
+        // (5) children onto the warp's stack while it has room, the rest to the ring
+        const bool split = have && v == kSplit;
+        const uint32_t splits = __ballot_sync(0xFFFFFFFFu, split);
+        const int made = 2 * __popc(splits);
+        delta += made - __popc(work);
+        const int room = kLocal - top;
+        const int r2 = 2 * __popc(splits & lt);
+        const uint64_t e0 = make_entry(row, depth + 1, path);
+        const uint64_t e1 = make_entry(row, depth + 1, path | (1u << depth));
+        bool out0 = false, out1 = false;
+        if (split) {
+            if (r2 < room) stk[top + r2] = e0;
+            else out0 = true;
+            if (r2 + 1 < room) stk[top + r2 + 1] = e1;
+            else out1 = true;
+        }
+        top += min(made, room);
+        __syncwarp();
+        if (__any_sync(0xFFFFFFFFu, out0 || out1)) {
+            if (lane == 0) atomicAdd(a.qPending, (unsigned long long)delta);
+            delta = 0;
+            if (!ring_push(a, out0, e0) || !ring_push(a, out1, e1)) {
+                failed = true;
+                break;
+            }
+        }
+        // (6) lend the oldest boxes (the shallowest: the most work) when the ring runs low
+        if (top > kDonateAbove && (kLendEvery == 1 || (++passes % kLendEvery) == 0)) {
+            int lend = 0;
+            if (lane == 0) {
+                const unsigned long long t = ld_volatile(a.qTail), h0 = ld_volatile(a.qHead);
+                lend = t < h0 + lowWater ? min(32, top / 2) : 0;
+            }
+            lend = __shfl_sync(0xFFFFFFFFu, lend, 0);
+            if (lend > 0) {
+                if (lane == 0) atomicAdd(a.qPending, (unsigned long long)delta);
+                delta = 0;
+                const uint64_t mine = lane < lend ? stk[lane] : 0ull;
+                __syncwarp();
+                for (int b = 0; b < top - lend; b += 32) {
+                    const int i = b + lane;
+                    const uint64_t x = i < top - lend ? stk[lend + i] : 0ull;
+                    __syncwarp();
+                    if (i < top - lend) stk[i] = x;
+                    __syncwarp();
+                }
+                top -= lend;
+                if (!ring_push(a, lane < lend, mine)) {
+                    failed = true;
+                    break;
+                }
+            }
+        }
+    }
+    if (failed && lane == 0) raise_error(a.status, kErrSpinLimit);
     if (a.stats) {
         warp_sum(a.stats + kStTested, tested);
         warp_sum(a.stats + kStCulled, culled);
@@ -937,19 +1214,40 @@ static cudaError_t sort_leaves(const SubArgs& a, uint64_t* fronts[2], size_t par
     return cudaSuccess;
 }
 
+#ifndef PZ_SUBDIV_ROUNDS
+#define PZ_SUBDIV_ROUNDS 0
+#endif
+
 template <int K>
 static cudaError_t run(SubArgs& a, uint64_t* fronts[2], size_t part, unsigned long long* counts, cudaStream_t s)
 {
     const int grid = num_sms() * 8;
-    k_sub_init<<<(a.nRows + kBlock - 1) / kBlock, kBlock, 0, s>>>(a, fronts[0], &counts[0]);
-    cudaError_t e = cudaGetLastError();
-    int cur = 0;
-    for (int d = 0; d <= a.maxDepth && e == cudaSuccess; d++) {
-        e = cudaMemsetAsync(&counts[cur ^ 1], 0, sizeof(unsigned long long), s);
-        if (e != cudaSuccess) break;
-        k_sub_round<K><<<grid, kBlock, 0, s>>>(a, d, fronts[cur], &counts[cur], fronts[cur ^ 1], &counts[cur ^ 1]);
+    cudaError_t e = cudaSuccess;
+    if (PZ_SUBDIV_ROUNDS) {
+        // one launch per depth over the whole frontier of that depth
+        k_sub_init<<<(a.nRows + kBlock - 1) / kBlock, kBlock, 0, s>>>(a, fronts[0], &counts[0]);
         e = cudaGetLastError();
-        cur ^= 1;
+        int cur = 0;
+        for (int d = 0; d <= a.maxDepth && e == cudaSuccess; d++) {
+            e = cudaMemsetAsync(&counts[cur ^ 1], 0, sizeof(unsigned long long), s);
+            if (e != cudaSuccess) break;
+            k_sub_round<K><<<grid, kBlock, 0, s>>>(a, d, fronts[cur], &counts[cur], fronts[cur ^ 1], &counts[cur ^ 1]);
+            e = cudaGetLastError();
+            cur ^= 1;
+        }
+    } else {
+        // one persistent launch over the box queue (the two frontier regions, contiguous)
+        a.ring = fronts[0];
+        a.ringCapacity = 2 * part / sizeof(uint64_t);
+        e = cudaMemsetAsync(a.ring, 0, 2 * part, s);
+        if (e != cudaSuccess) return e;
+        k_sub_queue_init<<<(a.nRows + kBlock - 1) / kBlock, kBlock, 0, s>>>(a);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        int perSM = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_sub_queue<K>, kBlock, 0);
+        if (e != cudaSuccess) return e;
+        k_sub_queue<K><<<num_sms() * std::max(perSM, 1), kBlock, 0, s>>>(a);
+        e = cudaGetLastError();
     }
     if (e != cudaSuccess) return e;
     e = sort_leaves(a, fronts, part, s);
@@ -969,10 +1267,10 @@ using namespace pz;
 using namespace pz::subdiv;
 
 static_assert(sizeof(pz_specular_root) == 64, "pz_specular_root layout");
-static_assert(56 + 8 * kNumStats <= 256, "stats fit the header");
+static_assert(56 + 8 * kNumStats <= 200, "stats fit the header before the queue words");
 
 namespace {
-constexpr size_t kHeader = 256;  // status | em1[2] | counts[2] | leaf, root, item counts | stats
+constexpr size_t kHeader = 256;  // status | em1[2] | counts[2] | leaf, root, item counts | stats | queue words
 }
 
 extern "C" size_t pz_subdivide_scratch_bytes(uint64_t box_capacity)
@@ -1057,6 +1355,11 @@ extern "C" int pz_subdivide_solve(int K, uint32_t events, pz_float3 p_beg, const
     a.rootCapacity = root_capacity;
     a.stats = stats;
     a.status = status;
+    a.qHead = reinterpret_cast<unsigned long long*>(base + 200);
+    a.qTail = reinterpret_cast<unsigned long long*>(base + 208);
+    a.qPending = reinterpret_cast<unsigned long long*>(base + 216);
+    a.ring = nullptr;
+    a.ringCapacity = 0;
 
     cudaError_t e = cudaMemsetAsync(base, 0, kHeader, s);
     if (e == cudaSuccess) {

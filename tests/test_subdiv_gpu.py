@@ -203,9 +203,11 @@ def test_host_checks():
 
 
 def test_capacity_overflow_is_reported():
-    """A root list or box list too small for the work is reported as PZ_ERR_DEVICE (the
+    """A root list or leaf list too small for the work is reported as PZ_ERR_DEVICE (the
     kernels drop what does not fit and set the capacity bit), and the counts still say how
-    many roots there were."""
+    many roots there were.  (The box queue itself needs little room: each warp keeps the
+    boxes of its tuples on its own stack, so a box capacity of one entry per tuple holds the
+    queue; the leaf list has the same capacity and overflows when the leaves outnumber it.)"""
     sc = S.lens_scene(side=8, seed=5, amplitude=0.05, events="T", width=16, height=16)
     t, at, b = _dev(sc)
     ends = torch.from_numpy(_ends(6, 2)).cuda()
@@ -219,9 +221,24 @@ def test_capacity_overflow_is_reported():
     small_roots = A.SubdivisionSolver(box_capacity=1 << 16, root_capacity=4)
     with pytest.raises(RuntimeError, match="capacity"):
         small_roots.run(1, ev, sc.p_light, ends, rows, etas, t, at, b, t)
-    small_boxes = A.SubdivisionSolver(box_capacity=rows.shape[0], root_capacity=1 << 12)
+    # a lens frame's work list has several leaves per tuple: a leaf list with room for one
+    # per tuple (the least scratch the solver accepts) overflows
+    fs = S.lens_scene(side=32, seed=1, events="T", width=48, height=48, n_bins=4)
+    ds = A.DeviceScene(fs)
+    frame = A.Frame(fs, path_capacity=1 << 20)
+    cache = A.PathCache(capacity=1 << 20, step=fs.cell_step)
+    A.solve_primary(ds, frame, iteration=0)
+    A.photon_trace(ds, cache, iteration=0)
+    nf = A.lookup_flatten(frame, cache, ev)
+    frows = A.work_list_rows(frame, cache, nf, 1)
+    fends = A.receiver_points(frame)
+    fetas = torch.from_numpy(fs.bin_etas()).cuda()
+    big = A.SubdivisionSolver(box_capacity=1 << 22, root_capacity=1 << 20)
+    _, _, _, stf = big.run(1, ev, fs.light_point(0), fends, frows, fetas, ds.tris, ds.attribs, ds.builder, ds.tris)
+    assert stf["leaves"] > 2 * nf
+    small_boxes = A.SubdivisionSolver(box_capacity=nf, root_capacity=1 << 20)
     with pytest.raises(RuntimeError, match="capacity"):
-        small_boxes.run(1, ev, sc.p_light, ends, rows, etas, t, at, b, t)
+        small_boxes.run(1, ev, fs.light_point(0), fends, frows, fetas, ds.tris, ds.attribs, ds.builder, ds.tris)
     # the solver stays usable after an overflow
     _, _, _, st2 = ok.run(1, ev, sc.p_light, ends, rows, etas, t, at, b, t)
     assert st2 == st
