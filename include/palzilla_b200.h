@@ -270,8 +270,9 @@ PZ_API int pz_solve_specular_plain(const pz_solve_desc* desc, pz_stream_t stream
  * queries, FP64 polish of ill-conditioned roots.  n_paths_dev (device u32, e.g. the
  * lookup counter) gives the item count on the device so no host round trip is needed
  * (desc->n_paths is then the capacity); NULL uses desc->n_paths.  blocks_per_sm <= 0
- * picks the default.  scratch: pz_solve_batched_scratch_bytes(K, capacity) bytes. */
-PZ_API size_t pz_solve_batched_scratch_bytes(int K, uint64_t max_paths);
+ * picks the default.  scratch: pz_solve_batched_scratch_bytes(K, capacity, n_bins) bytes (0 for
+ * K outside 1..4 or n_bins outside 1..64). */
+PZ_API size_t pz_solve_batched_scratch_bytes(int K, uint64_t max_paths, int n_bins);
 /* After a batched solve: the scratch header holds u64 diagnostics at byte offset 64:
  * items skipped by prediction, predicted, plain fallback, per-bin Newton solves, FP64
  * polishes, visibility-query overflows, visibility candidates, visibility queries,
@@ -309,12 +310,13 @@ PZ_API int pz_solve_constraints(int K, uint32_t events, pz_float3 p_beg, const i
  * (e.g. its lookup counter; NULL entries or a NULL array: descs[i].n_paths), descs[i].n_paths
  * its capacity.  pz_solve_specular_multi then only enqueues work (memsets and kernels), so
  * a frame that calls it can be captured in a CUDA graph.  Tuning: probe / phase-1 blocks per
- * SM, phase-2 blocks per SM (1 or 2) and records per phase-2 queue access; NULL = the best
- * found by pz_solve_multi_autotune for this (K, bins, capacity), else {8, 2, 1}.
+ * SM, phase-2 blocks per SM (1 or 2), and p2_chunk, which must be 1 (phase 2 takes one
+ * record per queue access); NULL = the best found by pz_solve_multi_autotune for this (K,
+ * bins, capacity), else {8, 2, 1}.
  * pz_solve_multi_autotune renders the batch once per candidate (clear the images after
  * it) and keeps the fastest. */
 typedef struct pz_batch_tuning { int p1_blocks_per_sm, p2_blocks_per_sm, p2_chunk; } pz_batch_tuning;
-PZ_API size_t pz_solve_multi_scratch_bytes(int K, uint32_t n_scenes, uint64_t max_paths_total);
+PZ_API size_t pz_solve_multi_scratch_bytes(int K, int n_bins, uint32_t n_scenes, uint64_t max_paths_total);
 PZ_API int pz_solve_multi_prepare(const pz_solve_desc* descs, const uint32_t* const* n_paths_dev, uint32_t n_scenes,
                                   void* scratch_dev, size_t scratch_bytes, pz_stream_t stream);
 PZ_API int pz_solve_specular_multi(int K, int n_bins, uint32_t n_scenes, uint64_t max_paths_total, void* scratch_dev,

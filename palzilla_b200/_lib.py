@@ -91,9 +91,9 @@ SIGNATURES = {
     "pz_reorder_specular_paths": (i32, [vp, vp, vp, u32, vp]),
     "pz_solve_specular_plain": (i32, [C.POINTER(SolveDesc), vp]),
     "pz_solve_constraints": (i32, [i32, u32, Float3, vp, vp, vp, u32, vp, vp, u32, i32, f32, i32, vp, vp, vp, vp]),
-    "pz_solve_batched_scratch_bytes": (sz, [i32, u64]),
+    "pz_solve_batched_scratch_bytes": (sz, [i32, u64, i32]),
     "pz_solve_specular_batched": (i32, [C.POINTER(SolveDesc), vp, vp, sz, i32, vp]),
-    "pz_solve_multi_scratch_bytes": (sz, [i32, u32, u64]),
+    "pz_solve_multi_scratch_bytes": (sz, [i32, i32, u32, u64]),
     "pz_solve_multi_prepare": (i32, [vp, vp, u32, vp, sz, vp]),
     "pz_solve_specular_multi": (i32, [i32, i32, u32, u64, vp, sz, vp, vp, vp]),
     "pz_solve_multi_autotune": (i32, [i32, i32, u32, u64, vp, sz, vp, vp, vp, vp]),

@@ -325,7 +325,7 @@ def solve_specular_plain(desc, stream=None):
 def solve_specular_batched(desc, scratch: Scratch, n_paths_dev=None, blocks_per_sm: int = 0, stream=None):
     """Batched persistent solve; n_paths_dev (device int32 tensor) supplies the item count
     on the device (desc.n_paths is then the capacity)."""
-    nbytes = _lib.lib().pz_solve_batched_scratch_bytes(desc.K, desc.n_paths)
+    nbytes = _lib.lib().pz_solve_batched_scratch_bytes(desc.K, desc.n_paths, desc.n_bins)
     buf = scratch.get(nbytes)
     _lib.call("pz_solve_specular_batched", C.byref(desc), _vp(n_paths_dev), _vp(buf), C.c_size_t(buf.numel()),
               C.c_int(blocks_per_sm), C.c_void_p(_stream(stream)))
@@ -477,7 +477,7 @@ class SceneBatch:
         self.total = sum(int(d.n_paths) for d in descs)
         self._descs = (_lib.SolveDesc * n)(*descs)
         self._counts = (C.c_void_p * n)(*[None if c is None else c.data_ptr() for c in (counts or [None] * n)])
-        nbytes = _lib.lib().pz_solve_multi_scratch_bytes(self.K, n, self.total)
+        nbytes = _lib.lib().pz_solve_multi_scratch_bytes(self.K, self.n_bins, n, self.total)
         self.scratch = torch.empty(nbytes, dtype=torch.uint8, device=device)
         _lib.call("pz_solve_multi_prepare", C.cast(self._descs, C.c_void_p), C.cast(self._counts, C.c_void_p),
                   C.c_uint32(n), _vp(self.scratch),

@@ -656,12 +656,14 @@ __global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
 
 // ---------------------------------------------------------------- phase 2
 // Phase 2 runs in waves of three kernels.  Each wave takes records (phase-1 items with bins
-// to solve) from the work counter while the accepted list has room for 64 more roots per
+// to solve) from the work counter while the accepted list has room for B more roots per
 // record (a record never has more), so any input fits in a fixed number of waves:
-//  * k_p2_solve, one warp per record: the lanes take the record's bins to solve in rank
-//    order (32 at a time, no lane idles for a bin the mask excludes); Newton, then
-//    admissibility; the accepted (converged and admissible) roots of each round are
-//    appended as one block {first, record, count};
+//  * k_p2_solve, persistent warps: the 32 lanes of a round take (record, bin) pairs, the
+//    bins of a record in rank order on consecutive lanes (a record solved bin by bin starts
+//    a round; predicted records are packed one after another); Newton, then
+//    admissibility; the accepted (converged and admissible) roots of a record leave as one
+//    block {first, record, count} (a per-warp stash joins the roots of a record split
+//    between two rounds);
 //  * k_p2_vis, one warp per block: the shadow segments of the block's roots share one
 //    fattened BVH query per path segment (all roots of a block belong to one record, so
 //    their segments are close); a root that is occluded gets throughput 0;
@@ -730,7 +732,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_p2_solve(BatchArgs a
         // the bins of a round mostly share one chain and one start and follow similar Newton
         // paths.  A predicted record is packed: its bins in rank order, then the next
         // record's, so no lane idles for a bin that a record's mask excludes.  A record is
-        // taken after reserving room for 64 accepted roots (a record never has more) in this
+        // taken after reserving room for B accepted roots (a record never has more) in this
         // wave.
         int filled = 0;
         unsigned long long myRec = 0;
@@ -741,7 +743,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_p2_solve(BatchArgs a
                 unsigned long long j = 0;
                 bool take = false;
                 if (lane == 0) {
-                    if (*a.workCounter < nRec && atomicAdd(reserved, 64ull) + 64ull <= a.acceptCapacity) {
+                    if (*a.workCounter < nRec && atomicAdd(reserved, (unsigned long long)B) + (unsigned long long)B <= a.acceptCapacity) {
                         j = atomicAdd(a.workCounter, 1ull);
                         take = j < nRec;
                     }

@@ -40,15 +40,15 @@ struct BatchArgs {
     int wave = 0;                      // phase-2 wave of this launch (0 .. kMaxWaves - 1)
 };
 
-// Phase 2 runs in at most kMaxWaves waves; each wave has room for 64 accepted roots (a record's
-// most) per record of 1/kMaxWaves of the record capacity, so every record fits.
+// Phase 2 runs in at most kMaxWaves waves; each wave has room for nBins accepted roots (a
+// record's most) per record of 1/kMaxWaves of the record capacity, so every record fits.
 constexpr int kMaxWaves = 8;
 // Relative determinant of an item's branch of roots below which the item is solved bin by bin
 // (near a fold of the caustic, where the prediction of the bins' roots is least reliable).
 constexpr float kDefaultFoldDet = 1.0e-2f;
-inline unsigned long long accept_capacity(unsigned long long recordCapacity)
+inline unsigned long long accept_capacity(unsigned long long recordCapacity, int nBins)
 {
-    return 64ull * ((recordCapacity + kMaxWaves - 1) / kMaxWaves);
+    return (unsigned long long)nBins * ((recordCapacity + kMaxWaves - 1) / kMaxWaves);
 }
 // at most three rounds (blocks) per record: B <= 64 bins on consecutive lanes of 32-lane
 // rounds that other records' bins may start and end

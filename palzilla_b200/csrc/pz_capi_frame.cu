@@ -239,22 +239,22 @@ struct BatchLayout {
     size_t records, probes, accepted, blocks, total;
 };
 inline size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
-BatchLayout batch_layout(int K, uint64_t maxPaths, size_t start)
+BatchLayout batch_layout(int K, uint64_t maxPaths, int nBins, size_t start)
 {
     BatchLayout L;
     L.records = start;
     L.probes = L.records + a256((size_t)maxPaths * batched::record_bytes(K));
     L.accepted = L.probes + a256((size_t)maxPaths * 3 * batched::probe_bytes(K));
-    L.blocks = L.accepted + a256((size_t)batched::accept_capacity(maxPaths) * batched::accepted_bytes(K));
+    L.blocks = L.accepted + a256((size_t)batched::accept_capacity(maxPaths, nBins) * batched::accepted_bytes(K));
     L.total = L.blocks + a256((size_t)batched::block_capacity(maxPaths) * batched::block_bytes());
     return L;
 }
 }  // namespace
 
-extern "C" size_t pz_solve_batched_scratch_bytes(int K, uint64_t max_paths)
+extern "C" size_t pz_solve_batched_scratch_bytes(int K, uint64_t max_paths, int n_bins)
 {
-    if (K < 1 || K > 4) return 0;
-    return batch_layout(K, max_paths, 256).total;
+    if (K < 1 || K > 4 || n_bins < 1 || n_bins > 64) return 0;
+    return batch_layout(K, max_paths, n_bins, 256).total;
 }
 
 extern "C" int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32_t* n_paths_dev, void* scratch_dev,
@@ -265,7 +265,7 @@ extern "C" int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32
     if (r != PZ_OK) return r;
     if (!desc->spectral || desc->n_bins < 1 || desc->n_bins > 64)
         return fail(PZ_ERR_INVALID_ARGUMENT, "pz_solve_specular_batched: binned mode with 1..64 bins required");
-    const size_t need = pz_solve_batched_scratch_bytes(desc->K, desc->n_paths);
+    const size_t need = pz_solve_batched_scratch_bytes(desc->K, desc->n_paths, desc->n_bins);
     if (!scratch_dev || scratch_bytes < need)
         return fail(PZ_ERR_SCRATCH_TOO_SMALL, "pz_solve_specular_batched: scratch %zu < required %zu", scratch_bytes,
                     need);
@@ -277,12 +277,12 @@ extern "C" int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32
     b.recordCount = reinterpret_cast<unsigned long long*>(base + 16);
     b.workCounter2 = reinterpret_cast<unsigned long long*>(base + 24);
     b.recordCount2 = reinterpret_cast<unsigned long long*>(base + 32);
-    const BatchLayout L = batch_layout(desc->K, desc->n_paths, 256);
+    const BatchLayout L = batch_layout(desc->K, desc->n_paths, desc->n_bins, 256);
     b.records = base + L.records;
     b.recordCapacity = desc->n_paths;
     b.probes = base + L.probes;
     b.accepted = base + L.accepted;
-    b.acceptCapacity = batched::accept_capacity(desc->n_paths);
+    b.acceptCapacity = batched::accept_capacity(desc->n_paths, desc->n_bins);
     b.blocks = base + L.blocks;
     b.blockCapacity = batched::block_capacity(desc->n_paths);
     b.p2 = reinterpret_cast<unsigned long long*>(base + 192);
@@ -326,12 +326,12 @@ inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 struct MultiLayout {
     size_t offsets, table, records, probes, accepted, blocks, total;
 };
-MultiLayout multi_layout(int K, uint32_t nScenes, uint64_t maxPaths)
+MultiLayout multi_layout(int K, int nBins, uint32_t nScenes, uint64_t maxPaths)
 {
     MultiLayout L;
     L.offsets = kMultiHeader;
     L.table = L.offsets + align256(8 * ((size_t)nScenes + 1));
-    const BatchLayout B = batch_layout(K, maxPaths, L.table + align256(sizeof(batched::SceneArgs) * (size_t)nScenes));
+    const BatchLayout B = batch_layout(K, maxPaths, nBins, L.table + align256(sizeof(batched::SceneArgs) * (size_t)nScenes));
     L.records = B.records;
     L.probes = B.probes;
     L.accepted = B.accepted;
@@ -351,10 +351,10 @@ std::tuple<int, int, int> tune_key(int K, int nBins, uint64_t maxPaths)
 }
 }  // namespace
 
-extern "C" size_t pz_solve_multi_scratch_bytes(int K, uint32_t n_scenes, uint64_t max_paths_total)
+extern "C" size_t pz_solve_multi_scratch_bytes(int K, int n_bins, uint32_t n_scenes, uint64_t max_paths_total)
 {
-    if (K < 1 || K > 4 || n_scenes == 0) return 0;
-    return multi_layout(K, n_scenes, max_paths_total).total;
+    if (K < 1 || K > 4 || n_bins < 1 || n_bins > 64 || n_scenes == 0) return 0;
+    return multi_layout(K, n_bins, n_scenes, max_paths_total).total;
 }
 
 extern "C" int pz_solve_multi_prepare(const pz_solve_desc* descs, const uint32_t* const* n_paths_dev, uint32_t n_scenes,
@@ -375,7 +375,7 @@ extern "C" int pz_solve_multi_prepare(const pz_solve_desc* descs, const uint32_t
         table[i].nPathsDev = n_paths_dev ? n_paths_dev[i] : nullptr;
         total += d.n_paths;
     }
-    const MultiLayout L = multi_layout(K, n_scenes, total);
+    const MultiLayout L = multi_layout(K, nb, n_scenes, total);
     if (!scratch_dev || scratch_bytes < L.total)
         return fail(PZ_ERR_SCRATCH_TOO_SMALL, "pz_solve_multi_prepare: scratch %zu < required %zu", scratch_bytes, L.total);
     if (reinterpret_cast<uintptr_t>(scratch_dev) & 255)
@@ -393,7 +393,7 @@ static int multi_args(int K, int n_bins, uint32_t n_scenes, uint64_t total, void
 {
     if (K < 1 || K > 4 || n_bins < 1 || n_bins > 64 || n_scenes == 0)
         return fail(PZ_ERR_INVALID_ARGUMENT, "%s: bad K / bins / scene count", who);
-    const MultiLayout L = multi_layout(K, n_scenes, total);
+    const MultiLayout L = multi_layout(K, n_bins, n_scenes, total);
     if (!scratch_dev || scratch_bytes < L.total)
         return fail(PZ_ERR_SCRATCH_TOO_SMALL, "%s: scratch %zu < required %zu", who, scratch_bytes, L.total);
     char* base = static_cast<char*>(scratch_dev);
@@ -410,7 +410,7 @@ static int multi_args(int K, int n_bins, uint32_t n_scenes, uint64_t total, void
     b->recordCapacity = total;
     b->probes = base + L.probes;
     b->accepted = base + L.accepted;
-    b->acceptCapacity = batched::accept_capacity(total);
+    b->acceptCapacity = batched::accept_capacity(total, n_bins);
     b->blocks = base + L.blocks;
     b->blockCapacity = batched::block_capacity(total);
     b->p2 = reinterpret_cast<unsigned long long*>(base + 192);
@@ -454,7 +454,7 @@ extern "C" int pz_solve_specular_multi(int K, int n_bins, uint32_t n_scenes, uin
         if (it != g_tunings.end()) t = it->second;
     }
     if (t.p1_blocks_per_sm < 1 || t.p1_blocks_per_sm > 32 || t.p2_blocks_per_sm < 1 || t.p2_blocks_per_sm > 2 ||
-        t.p2_chunk < 1 || t.p2_chunk > 64)
+        t.p2_chunk != 1)
         return fail(PZ_ERR_INVALID_ARGUMENT, "pz_solve_specular_multi: tuning out of range");
     return done(run_multi(K, b, t, offsets, scratch_dev, S(stream)), "pz_solve_specular_multi");
 }

@@ -201,7 +201,8 @@ def test_batched_host_checks():
     spectral = torch.zeros((sc.width * sc.height, sc.n_bins), device="cuda")
     etas = torch.from_numpy(sc.bin_etas()).cuda()
     s = C.c_void_p(torch.cuda.current_stream().cuda_stream)
-    need = L.pz_solve_batched_scratch_bytes(1, n)
+    need = L.pz_solve_batched_scratch_bytes(1, n, sc.n_bins)
+    assert L.pz_solve_batched_scratch_bytes(1, n, 0) == 0 and L.pz_solve_batched_scratch_bytes(1, n, 65) == 0
     small = torch.empty(need - 256, dtype=torch.uint8, device="cuda")
     d = A.solve_desc(ds, frame, cache, sc.events, n, spectral=spectral, etas=etas)
     r = L.pz_solve_specular_batched(C.byref(d), None, C.c_void_p(small.data_ptr()), C.c_size_t(small.numel()), 0, s)
