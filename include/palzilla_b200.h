@@ -390,9 +390,12 @@ typedef struct pz_specular_root {
     float throughput; /* contributableThroughput, > 0 */
     uint32_t pad[3];
 } pz_specular_root;   /* 64 bytes */
-/* Scratch: a 256-byte header, two box frontiers and the leaf list of box_capacity entries
- * each (box_capacity >= n_tuples); the frontiers then hold the (leaf, bin) solve list
- * (2 * box_capacity entries). */
+/* Scratch: a 256-byte header, a box queue of 2 * box_capacity entries and the leaf list of
+ * box_capacity entries (box_capacity >= n_tuples).  All depths are bounded in one persistent
+ * kernel: each warp keeps the boxes of its tuples on a stack in shared memory and the queue
+ * (a ring in the scratch) holds the tuples, the boxes a stack cannot take and the boxes
+ * lent to idle warps, so it needs little room; the leaf list must hold every leaf.  The
+ * queue's space then holds the (leaf, bin) solve list (2 * box_capacity entries). */
 PZ_API size_t pz_subdivide_scratch_bytes(uint64_t box_capacity);
 /* Writes the kept roots (unordered) to roots_dev and their count (which may exceed
  * root_capacity: PZ_ERR_DEVICE is then returned) to *n_roots_out.  Synchronises `stream`
