@@ -227,6 +227,38 @@ __global__ void __launch_bounds__(kBlock) k_build(Node* __restrict__ nodes, uint
     uint32_t pc[2], pctx = 0;
     Box pb[2];
     bool isRoot = true;
+    // A node whose children are both leaves (leaf i climbs right, leaf i + 1 climbs left: a
+    // local maximum of the deltas, about a third of the nodes of random keys) is made by
+    // leaf i's thread alone, with the box of leaf i + 1 from its triangle; leaf i + 1's
+    // thread stops.  The node is the one the handshake would make (same children, boxes,
+    // parent and escape link), without its pending slots and flag exchange.
+    if (nInternals > 0) {
+        const auto goes_left = [&](uint32_t l) {
+            const uint32_t a = 0 < l ? __ldg(deltas + l - 1) : 0xFFFFFFFFu;
+            const uint32_t b = l < nInternals ? __ldg(deltas + l) : 0xFFFFFFFFu;
+            return a < b;
+        };
+        const bool left = goes_left(i_leaf);
+        if (!left && goes_left(i_leaf + 1)) {
+            const uint32_t tri1 = (uint32_t)(sorted[i_leaf + 1] >> 32);
+            const float* t1 = reinterpret_cast<const float*>(tris) + (size_t)tri1 * 9;
+            Box b1 = box_empty();
+            box_extend(b1, mk3(__ldg(t1 + 0), __ldg(t1 + 1), __ldg(t1 + 2)));
+            box_extend(b1, mk3(__ldg(t1 + 3), __ldg(t1 + 4), __ldg(t1 + 5)));
+            box_extend(b1, mk3(__ldg(t1 + 6), __ldg(t1 + 7), __ldg(t1 + 8)));
+            pc[0] = node;
+            pc[1] = make_node(tri1, true);
+            pb[0] = box;
+            pb[1] = b1;
+            upper = i_leaf + 1;
+            pctx = upper < nInternals ? upper : 0xFFFFFFFFu;
+            pending = true;
+            node = make_node(i_leaf, false);
+            box_extend(box, b1);
+        } else if (left && i_leaf > 0 && !goes_left(i_leaf - 1)) {
+            return;  // leaf i - 1's thread makes the parent
+        }
+    }
     while (upper - lower < nInternals) {
         const uint32_t dL = 0 < lower ? __ldg(deltas + lower - 1) : 0xFFFFFFFFu;
         const uint32_t dR = upper < nInternals ? __ldg(deltas + upper) : 0xFFFFFFFFu;
