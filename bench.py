@@ -339,10 +339,11 @@ def run_ours(args):
 
     sort_build = bench_sort_build(hbm, hbm_kind) if (rank == 0 and not args.no_sort) else None
 
-    cpu = fp64 = None
+    cpu = fp64 = flops = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(R, seconds=args.cpu_seconds)
         fp64 = fp64_error(R)
+        flops = newton_flops(R, counters, solve_avg, clk.get("sm_mhz") or 1965.0, sms)
 
     if rank == 0:
         line = {
@@ -374,6 +375,7 @@ def run_ours(args):
                            "kernel's"),
             "image_rel_rmse": rmse,
             "fp64_error": fp64,
+            "fp32_flops": flops,
             "batched_counters": counters,
             "e2e": {"value": e2e_paths / (e2e_ms / 1e3), "unit": UNIT, "steps": ke, "ms_per_step": e2e_ms / ke,
                     "h2d_bytes_per_step": int(tris_h.numel() * 4 + att_h.numel()),
@@ -880,6 +882,35 @@ def fp64_error(R, n=100000):
     return {"batched_vs_fp64": rel(gpu, img64), "oracle_fp32_vs_fp64": rel(img32, img64),
             "batched_vs_oracle_fp32": rel(gpu, img32),
             "sample": f"{len(sel)} of the frame's {m} work items x {sc.n_bins} bins, spectral image rel. RMSE"}
+
+
+def newton_flops(R, counters, solve_ms, sm_mhz, sms):
+    """FP32 operations of the solve stage's Newton iterations: one iteration of the
+    restated solveConstraints<2> (the reference's algorithm: 2K single-tangent dual
+    evaluations, Householder QR, update) counted with a counting scalar type on the
+    frame's first work item's chain, times the Newton iterations phase 2 ran, over the
+    solve stage's time.  The probes' and phase 1's iterations are not in the count, so the
+    figure is a lower bound.  Peak: 128 FP32 lanes x 148 SMs x 2 (FMA) x the SM clock; the
+    solver units are built without FMA contraction, so one lane does one operation a clock
+    and half that peak is their ceiling."""
+    import oracle as O
+    from palzilla_b200.scenes import event_descriptor
+    sc = R.sc
+    pairs = R.frame.paths[:8].cpu().numpy().view(np.int32).reshape(-1, 2)
+    px, slot = int(pairs[0, 0]), int(pairs[0, 1])
+    cache = R.cache.to_host()
+    fd = R.frame.fd[px * 40:(px + 1) * 40].cpu().numpy().view(np.float32)
+    tup = cache["tris"][slot, :2]
+    c = O.oracle().count_newton_flops(2, cache["params"][slot, :4], sc.light_point(R.iteration), fd[:3],
+                                      sc.tris[tup], sc.attribs[tup], float(sc.bin_etas()[sc.n_bins // 2]),
+                                      event_descriptor(sc.events))
+    iters = float(counters["newton_iterations"])
+    achieved = c["total"] * iters / (solve_ms / 1e3) / 1e9
+    peak = 128 * sms * 2 * sm_mhz * 1e6 / 1e9
+    return {"per_newton_iteration": c, "newton_iterations": iters, "achieved": achieved, "peak": peak,
+            "unit": "GFLOP/s", "frac": achieved / peak,
+            "note": "phase-2 Newton iterations only (a lower bound); peak with FMA, the solver units run "
+                    "without contraction (ceiling half of it)"}
 
 
 def cpu_stages(R, lib, kind, solve_paths_per_s, reps=5):

@@ -226,6 +226,21 @@ class CpuLib:
         return accum, fd
 
     # ------------------------------------------------------------------ solver primitives
+    def count_newton_flops(self, K, params, p_beg, p_end, tris, attribs, eta, ev):
+        """Floating-point operations of one Newton iteration of the restated
+        solveConstraints<K> (pk.h:466-592), counted with a counting scalar type (oracle
+        library only): {"add", "mul", "div", "sqrt", "total"}."""
+        out = np.zeros(4, np.uint64)
+        r = self.f("count_newton_flops", C.c_int)(
+            C.c_int(K), _p(np.ascontiguousarray(params, np.float32)), _p(np.asarray(p_beg, np.float32)),
+            _p(np.asarray(p_end, np.float32)), _p(np.ascontiguousarray(tris, np.float32)),
+            _p(np.ascontiguousarray(attribs)), C.c_float(eta), C.c_uint32(ev), _p(out))
+        if r != 0:
+            raise ValueError("K must be 1..4")
+        c = dict(zip(("add", "mul", "div", "sqrt"), (int(v) for v in out)))
+        c["total"] = sum(c.values())
+        return c
+
     def solve_constraints(self, K, params, p_beg, p_end, tris, attribs, eta, ev, max_iter=32, tol=1e-10, warmup=1,
                           dtype=np.float32):
         prm = np.array(params, dtype)

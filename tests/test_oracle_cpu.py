@@ -310,3 +310,22 @@ def test_subdivision_directed_rounding_is_exact(orc):
         assert Fraction(d) ** 2 <= Fraction(x) <= Fraction(u) ** 2
         assert u == d or u == float(np.nextafter(np.float32(d), np.float32(np.inf)))
         assert (u == d) == (Fraction(d) ** 2 == Fraction(x))
+
+
+def test_newton_flop_count(orc):
+    """The operation count of one Newton iteration of the restated solver (a counting scalar
+    type; used by the bench line's FP32 figure) is positive, the same on every call, and grows
+    with the chain: 2K dual evaluations of K vertices, then a 3K x 2K least-squares step."""
+    sc = S.lens_scene(side=16, seed=1, events="TT")
+    spec = np.nonzero(sc.attribs["material"] != 0)[0]
+    tup = [spec[0], spec[len(spec) // 2 + 3]]
+    counts = {}
+    for K, ev in ((1, "T"), (2, "TT")):
+        args = (K, np.full(2 * K, 0.3, np.float32), sc.p_light, (0.0, 0.0, 0.0), sc.tris[tup[:K]],
+                sc.attribs[tup[:K]], 1.5, S.event_descriptor(ev))
+        c = orc.count_newton_flops(*args)
+        assert c == orc.count_newton_flops(*args)
+        assert c["add"] > 0 and c["mul"] > 0 and c["div"] > 0 and c["sqrt"] > 0
+        assert c["total"] == c["add"] + c["mul"] + c["div"] + c["sqrt"]
+        counts[K] = c["total"]
+    assert 3 * counts[1] < counts[2] < 5 * counts[1], counts
