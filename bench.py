@@ -337,6 +337,7 @@ def run_ours(args):
                 "note": "the stage is issue-bound (FP32 Newton/QR and BVH queries in registers, scene and BVH in "
                         "L2): its HBM fraction is small by design, its issue fraction is the bound"}
 
+    stages = frame_stages(R)
     sort_build = bench_sort_build(hbm, hbm_kind) if (rank == 0 and not args.no_sort) else None
 
     cpu = fp64 = flops = None
@@ -363,6 +364,7 @@ def run_ours(args):
                         "solved) over the solve stage's time; value counts every (item, bin) decided, as the "
                         "plain path decides each by a Newton solve"},
             "solve_ms_per_frame": solve_avg,
+            "frame_stages": stages,
             "plain": {"value": p_value, "ms_per_frame": p_tmax / kp, "solve_ms_per_frame": float(np.mean(p_solve_ms)),
                       "steps": kp},
             "speedup_paths_per_s_vs_plain": value / p_value,
@@ -392,6 +394,39 @@ def run_ours(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def frame_stages(R, first=300, frames=3):
+    """CUDA-event times of a frame's stages before the solve (median over `frames` frames):
+    eye pass (primary and shadow rays), photon pass, lookup/flatten with the count read back,
+    tuple sort and reorder; with rays/s and photons/s."""
+    import torch
+    A, fr, sc = R.A, R.frame, R.sc
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+    t = {"eye_pass": [], "photon_pass": [], "lookup": [], "sort_reorder": []}
+    for i in range(frames):
+        e = [ev() for _ in range(5)]
+        torch.cuda.synchronize()
+        e[0].record()
+        A.solve_primary(R.ds, fr, iteration=first + i)
+        e[1].record()
+        R.cache.clear()
+        A.photon_trace(R.ds, R.cache, iteration=first + i)
+        e[2].record()
+        n = A.lookup_flatten(fr, R.cache, R.ev)
+        e[3].record()
+        A.sort_and_reorder(fr, n, R.sorter)
+        e[4].record()
+        torch.cuda.synchronize()
+        for k, (a, b) in zip(t, zip(e[:-1], e[1:])):
+            t[k].append(a.elapsed_time(b))
+    ms = {k: float(np.median(v)) for k, v in t.items()}
+    photons = sc.n * sc.photons_per_triangle
+    return {"ms": ms, "primary_rays_per_s": sc.width * sc.height / (ms["eye_pass"] / 1e3),
+            "photons_per_s": photons / (ms["photon_pass"] / 1e3),
+            "note": "each pixel: one primary ray and a shadow ray; each photon: up to 5 closest-hit rays"}
 
 
 def reference_gpu_solve(R, steps=2):
