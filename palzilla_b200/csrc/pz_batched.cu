@@ -464,7 +464,7 @@ PZ_D void flush_count(unsigned long long* counter, unsigned long long v)
 }
 
 template <int K, bool kMulti>
-__global__ void __launch_bounds__(256, 2) k_phase1(BatchArgs a)
+__global__ void __launch_bounds__(256, kPhase1Blocks) k_phase1(BatchArgs a)
 {
     const int B = a.s.nBins;
     const uint64_t nPaths = total_items<kMulti>(a);
@@ -701,7 +701,7 @@ PZ_D unsigned long long drop_low_bits(unsigned long long m, int n)
 }
 
 template <int K, bool kMulti>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_p2_solve(BatchArgs a)
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, kP2SolveBlocks) k_p2_solve(BatchArgs a)
 {
     const int lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;

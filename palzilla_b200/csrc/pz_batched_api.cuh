@@ -43,6 +43,15 @@ struct BatchArgs {
 // Phase 2 runs in at most kMaxWaves waves; each wave has room for nBins accepted roots (a
 // record's most) per record of 1/kMaxWaves of the record capacity, so every record fits.
 constexpr int kMaxWaves = 8;
+// blocks per SM the phase-1 and phase-2 solve kernels are built for (register budget)
+#ifndef PZ_P2_SOLVE_BLOCKS
+#define PZ_P2_SOLVE_BLOCKS 2
+#endif
+#ifndef PZ_PHASE1_BLOCKS
+#define PZ_PHASE1_BLOCKS 2
+#endif
+constexpr int kP2SolveBlocks = PZ_P2_SOLVE_BLOCKS;
+constexpr int kPhase1Blocks = PZ_PHASE1_BLOCKS;
 // Relative determinant of an item's branch of roots below which the item is solved bin by bin
 // (near a fold of the caustic, where the prediction of the bins' roots is least reliable).
 constexpr float kDefaultFoldDet = 1.0e-2f;

@@ -295,7 +295,8 @@ extern "C" int pz_solve_specular_batched(const pz_solve_desc* desc, const uint32
     b.illDet = desc->fold_det < 0.0f ? 0.0f : (desc->fold_det == 0.0f ? batched::kDefaultFoldDet : desc->fold_det);
     if (desc->n_paths == 0) { clear_error(); return PZ_OK; }
     cudaError_t e = cudaMemsetAsync(base, 0, 256, S(stream));
-    if (e == cudaSuccess) e = batched::launch_solve_batched(desc->K, b, blocks_per_sm > 0 ? blocks_per_sm : 2, S(stream));
+    if (e == cudaSuccess) e = batched::launch_solve_batched(desc->K, b, blocks_per_sm > 0 ? blocks_per_sm : batched::kP2SolveBlocks,
+                                                        S(stream));
     return done(e, "pz_solve_specular_batched");
 }
 
