@@ -133,20 +133,27 @@ def setup_dist():
 
 
 def barrier(world):
+    """Every rank's device work done, then a process-group barrier (nccl on the GPUs; the
+    host-side logic also runs on gloo, without a device)."""
     import torch
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
-        torch.cuda.synchronize()
+        if torch.cuda.is_available():
+            torch.cuda.synchronize()
 
 
 def reduce(world, v: float, op: str) -> float:
+    """max or sum of a per-rank figure over the ranks (value = all ranks' path solves over the
+    slowest rank's device time)."""
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], device="cuda", dtype=torch.float64)
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], device=device, dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
 
