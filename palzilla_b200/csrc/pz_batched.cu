@@ -463,6 +463,10 @@ PZ_D void flush_count(unsigned long long* counter, unsigned long long v)
     if ((threadIdx.x & 31) == 0 && v) atomicAdd(counter, v);
 }
 
+#ifndef PZ_PHASE1_PROBE_START
+#define PZ_PHASE1_PROBE_START 1
+#endif
+
 template <int K, bool kMulti>
 __global__ void __launch_bounds__(256, kPhase1Blocks) k_phase1(BatchArgs a)
 {
@@ -502,6 +506,17 @@ __global__ void __launch_bounds__(256, kPhase1Blocks) k_phase1(BatchArgs a)
 #pragma unroll
             for (int i = 0; i < 2 * K; i++) x[i] = xpc[i];
         } else {
+#if PZ_PHASE1_PROBE_START
+            // the centre probe's last iterate (two Newton steps from the photon's start, where
+            // its edge test stopped it) starts the unconstrained solve, when it is finite
+            bool usable = true;
+#pragma unroll
+            for (int i = 0; i < 2 * K; i++) usable = usable && fabsf(xpc[i]) < 1.0e3f;
+            if (usable) {
+#pragma unroll
+                for (int i = 0; i < 2 * K; i++) x[i] = xpc[i];
+            }
+#endif
             conv = newton_nl<K>(x, ch, S.p_light, S.fds[sp.pixel].p, eta_c, S.events, 24, S.costTolerance, 0, false, 0,
                                 &det);
         }
