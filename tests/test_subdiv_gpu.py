@@ -77,6 +77,42 @@ def test_single_refraction_all_triangles_matches_oracle(orc, amplitude, side, bi
           f"roots {st['roots']}")
 
 
+@pytest.mark.parametrize("max_depth,eps", [(0, 1e-4), (5, 1e-4), (16, 0.0)])
+def test_uneven_depths_in_one_queue_match_oracle(orc, max_depth, eps):
+    """Rows of a rough lens (many boxes deep) mixed with rows of a smooth one (most die at
+    depth 0) in one persistent launch, with the box queue at its smallest (one entry per
+    tuple): the warps' stacks hold the deep tuples' boxes, lending them to the queue as
+    other warps run dry.  Roots and statistics equal the oracle's at every depth limit."""
+    rough = S.lens_scene(side=8, seed=3, amplitude=0.05, events="T", width=16, height=16)
+    smooth = S.lens_scene(side=24, seed=4, amplitude=0.005, events="T", width=16, height=16)
+    # one soup: the rough lens's specular triangles, then the smooth lens's
+    sr = np.nonzero(rough.attribs["material"] != 0)[0]
+    ss = np.nonzero(smooth.attribs["material"] != 0)[0]
+    tris = np.concatenate([rough.tris[sr], smooth.tris[ss]])
+    attribs = np.concatenate([rough.attribs[sr], smooth.attribs[ss]])
+    ends = _ends(8, 13)
+    rows = np.array([[q, i] for q in range(len(ends)) for i in range(len(tris))], np.int32)
+    t = torch.from_numpy(np.ascontiguousarray(tris, np.float32)).cuda()
+    at = torch.from_numpy(np.ascontiguousarray(attribs).view(np.uint8).reshape(-1)).cuda()
+    scene_t = torch.from_numpy(np.ascontiguousarray(rough.tris, np.float32)).cuda()
+    b = A.BVHGPUBuilder()
+    b.build(scene_t, scene_t.shape[0], 0)
+    etas = np.array([1.5, 1.55], np.float32)
+    ev = S.event_descriptor("T")
+    solver = A.SubdivisionSolver(box_capacity=len(rows), root_capacity=1 << 18, max_depth=max_depth, eps=eps)
+    ids, params, thr, st = solver.run(1, ev, rough.p_light, torch.from_numpy(ends).cuda(), torch.from_numpy(rows).cuda(),
+                                      torch.from_numpy(etas).cuda(), t, at, b, scene_t)
+    torch.cuda.synchronize()
+    ids, params, thr = _sorted(ids, params, thr)
+    bo = orc.build_bvh(rough.tris, 0)
+    exp, est = orc.subdivide_solve(1, ev, rough.p_light, ends, rows, etas, tris, attribs, bo, rough.tris,
+                                   max_depth=max_depth, eps=eps, cap=1 << 18)
+    _check_equal(exp, ids, params, thr, 1)
+    assert [st[k] for k in STAT_KEYS] == est.tolist()
+    print(f"\nmax depth {max_depth}: rows {len(rows)}, boxes {st['boxes_tested']}, leaves {st['leaves']}, "
+          f"roots {st['roots']}")
+
+
 def test_two_refractions_path_cuts_rows_match_oracle(orc):
     """Rows from Path Cuts (directed rounding) over the lens's specular triangles, K = 2."""
     sc = S.lens_scene(side=12, seed=5, events="TT", width=16, height=16)
