@@ -503,12 +503,24 @@ def bench_sort_build(hbm, hbm_kind, n=1 << 24):
     tris = torch.from_numpy(S.random_soup(n, seed=1001)).cuda()
     b = BVHGPUBuilder()
     build_ms = med(lambda: b.build(tris, n, 0))
+    # the reference's own LBVH kernels (getSceneAABB, buildMortons, computeDeltas, build;
+    # minimum_lbvh.cu:6-120, built from its sources for sm_100a) on the same triangles, with
+    # this library's sort between them (the reference's onesweep reorder is not run: it takes
+    # its tile from blockIdx.x and waits on its predecessors without a bound)
+    ref_build = None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_gpu as G
+    if G.available("default"):
+        rg = G.RefGpu("default")
+        ref_build = {"ms": med(lambda: rg.bvh_build(tris, n, lambda k, t, m: sorter.sort(k, None, t, None, m, 0, 32))),
+                     "kernels": "the reference's minimum_lbvh.cu kernels (default build) + this library's sort"}
+        ref_build["speedup"] = ref_build["ms"] / build_ms
     sort_gbs = 72.0 * n / (sort_ms / 1e3) / 1e9
     build_gbs = (189.0 + 72.0) * n / (build_ms / 1e3) / 1e9
     return {"n": n, "sort_ms": sort_ms, "keys_per_s": n / (sort_ms / 1e3),
             "sort_roofline": {"bound": "hbm", "achieved": sort_gbs, "peak": hbm, "unit": "GB/s",
                               "frac": sort_gbs / hbm, "peak_kind": hbm_kind, "bytes_per_key": 72},
-            "build_ms": build_ms, "triangles_per_s": n / (build_ms / 1e3),
+            "build_ms": build_ms, "triangles_per_s": n / (build_ms / 1e3), "reference_gpu_build": ref_build,
             "build_roofline": {"bound": "hbm", "achieved": build_gbs, "peak": hbm, "unit": "GB/s",
                                "frac": build_gbs / hbm, "peak_kind": hbm_kind, "bytes_per_triangle": 261}}
 
