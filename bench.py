@@ -344,7 +344,7 @@ def run_ours(args):
                 "note": "the stage is issue-bound (FP32 Newton/QR and BVH queries in registers, scene and BVH in "
                         "L2): its HBM fraction is small by design, its issue fraction is the bound"}
 
-    stages = frame_stages(R)
+    stages = frame_stages(R, with_reference=rank == 0 and world == 1 and not args.no_ref_gpu)
     sort_build = bench_sort_build(hbm, hbm_kind) if (rank == 0 and not args.no_sort) else None
 
     cpu = fp64 = flops = None
@@ -403,7 +403,7 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def frame_stages(R, first=300, frames=3):
+def frame_stages(R, first=300, frames=3, with_reference=False):
     """CUDA-event times of a frame's stages before the solve (median over `frames` frames):
     eye pass (primary and shadow rays), photon pass, lookup/flatten with the count read back,
     tuple sort and reorder; with rays/s and photons/s."""
@@ -431,9 +431,48 @@ def frame_stages(R, first=300, frames=3):
             t[k].append(a.elapsed_time(b))
     ms = {k: float(np.median(v)) for k, v in t.items()}
     photons = sc.n * sc.photons_per_triangle
-    return {"ms": ms, "primary_rays_per_s": sc.width * sc.height / (ms["eye_pass"] / 1e3),
-            "photons_per_s": photons / (ms["photon_pass"] / 1e3),
-            "note": "each pixel: one primary ray and a shadow ray; each photon: up to 5 closest-hit rays"}
+    out = {"ms": ms, "primary_rays_per_s": sc.width * sc.height / (ms["eye_pass"] / 1e3),
+           "photons_per_s": photons / (ms["photon_pass"] / 1e3),
+           "note": "each pixel: one primary ray and a shadow ray; each photon: up to 5 closest-hit rays"}
+    if with_reference:
+        out["reference_gpu_photon_pass"] = reference_gpu_photons(R, first, frames)
+        ref = out["reference_gpu_photon_pass"]
+        if "photons_per_s" in ref:
+            ref["speedup_photons_per_s"] = out["photons_per_s"] / ref["photons_per_s"]
+    return out
+
+
+def reference_gpu_photons(R, first, frames):
+    """The reference's photonTrace (main_gpu.cu:56-211, its sources built for sm_100a): one
+    256-thread block per triangle (256 photons each, its fixed block size) into its own
+    PathCache, on the same scene, BVH and light samples; median of `frames` launches."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_gpu as G
+    if not G.available("default"):
+        return {"unavailable": "reference GPU kernels not built (oracle/build_ref_gpu.sh needs the reference sources)"}
+    rg = G.RefGpu("default")
+    sc = R.sc
+    rc = rg.new_cache()
+    stack = rg.new_stack()
+    emin, emax = sc.eta_range()
+    ts = []
+    for i in range(frames + 1):
+        rc["hashes"].zero_()
+        rc["count"].zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        rg.photon_trace(rc, R.ds.internals, R.ds.root_dev, R.ds.tris, R.ds.attribs, R.ds.n, sc.light_point(first + i),
+                        emin, emax, first + i, sc.cell_step, sc.min_throughput, stack)
+        e1.record()
+        torch.cuda.synchronize()
+        if i > 0:
+            ts.append(e0.elapsed_time(e1))
+    ms = float(np.median(ts))
+    photons = sc.n * 256
+    del stack, rc
+    return {"ms": ms, "photons": photons, "photons_per_s": photons / (ms / 1e3),
+            "kernel": "photonTrace (main_gpu.cu:56-211), default build, 256 photons per triangle"}
 
 
 def reference_gpu_solve(R, steps=2):
