@@ -936,139 +936,160 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 3) k_p2_vis(BatchArgs a)
     const auto* blocks = reinterpret_cast<const AcceptBlock*>(a.blocks);
     unsigned long long cQueries = 0, cOverflow = 0, cCand = 0;
     for (;;) {
+        // Blocks are taken in pairs.  Two blocks of one tuple (consecutive records: the work
+        // list is in tuple order, so neighbouring pixels) whose roots fit the warp share one
+        // query, fattened to cover both; otherwise the warp runs them one after the other.
         unsigned long long bi = 0;
-        if (lane == 0) bi = atomicAdd(a.p2 + 3, 1ull);
+        if (lane == 0) bi = atomicAdd(a.p2 + 3, 2ull);
         bi = __shfl_sync(0xFFFFFFFFu, bi, 0);
         if (bi >= nB) break;
-        const AcceptBlock blk = blocks[bi];
-        const PairRec<K>& r = recs[blk.rec];
-        const SolveArgs& S = kMulti ? a.scenes[r.scene].s : a.s;
-        const uint32_t root = __ldg(S.root);
-        const int4 ti = S.cache.tris[r.slot];
-        const int tix[4] = {ti.x, ti.y, ti.z, ti.w};
-        Chain<K> ch;
-        load_chain<K>(ch, S.tris, S.attribs, tix);
-        const float3 pe = S.fds[r.pixel].p;
-        const bool mine = (uint32_t)lane < blk.count;
-        float thr = 0.0f;
-        float xs[2 * K];
-        if (mine) {
-            const Accepted<K>& e = acc[blk.first + lane];
-            thr = e.thr;
-#pragma unroll
-            for (int i = 0; i < 2 * K; i++) xs[i] = e.x[i];
+        const AcceptBlock b0 = blocks[bi];
+        const bool has1 = bi + 1 < nB;
+        const AcceptBlock b1 = has1 ? blocks[bi + 1] : AcceptBlock{0u, b0.rec, 0u};
+        bool merge = false;
+        if (has1 && b0.count + b1.count <= 32u) {
+            const PairRec<K>& r0 = recs[b0.rec];
+            const PairRec<K>& r1 = recs[b1.rec];
+            merge = r0.slot == r1.slot && r0.scene == r1.scene;
         }
-        // the shadow segments of every root: endpoints are the chain's vertices and shading
-        // normals (contributableThroughput, pk.h:763-789), offset as occluded() does
-        float3 sa[NS], sd[NS];
-#pragma unroll
-        for (int sg = 0; sg < NS; sg++) sa[sg] = sd[sg] = mk3(0.f, 0.f, 0.f);
-        if (thr > 0.0f) {
-            float3 va, na;
-            chain_vertex<K>(ch, xs, S.p_light, pe, 0, va, na);
-#pragma unroll
-            for (int sg = 0; sg < NS; sg++) {
-                float3 vb, nb, b;
-                chain_vertex<K>(ch, xs, S.p_light, pe, sg + 1, vb, nb);
-                shadow_segment(va, na, vb, nb, sa[sg], b);
-                sd[sg] = ex::sub3(b, sa[sg]);
-                va = vb;
-                na = nb;
+        const int units = merge ? 1 : (has1 ? 2 : 1);
+        for (int unit = 0; unit < units; unit++) {
+            // this lane's block and its root's index in it
+            AcceptBlock blk = unit == 0 ? b0 : b1;
+            uint32_t idx = (uint32_t)lane;
+            if (merge && (uint32_t)lane >= b0.count) {
+                blk = b1;
+                idx = (uint32_t)lane - b0.count;
             }
-        }
-        const uint32_t valid = __ballot_sync(0xFFFFFFFFu, thr > 0.0f);
-        if (valid) {
-            // one merged query for all segments, each fattened to cover every root's segment
-            const int leader = __ffs(valid) - 1;
-            float3 ra[NS], rinv[NS];
-            float rad[NS];
+            const PairRec<K>& r = recs[blk.rec];
+            const SolveArgs& S = kMulti ? a.scenes[r.scene].s : a.s;
+            const uint32_t root = __ldg(S.root);
+            const int4 ti = S.cache.tris[r.slot];
+            const int tix[4] = {ti.x, ti.y, ti.z, ti.w};
+            Chain<K> ch;
+            load_chain<K>(ch, S.tris, S.attribs, tix);
+            const float3 pe = S.fds[r.pixel].p;
+            const bool mine = idx < blk.count;
+            float thr = 0.0f;
+            float xs[2 * K];
+            if (mine) {
+                const Accepted<K>& e = acc[blk.first + idx];
+                thr = e.thr;
 #pragma unroll
-            for (int sg = 0; sg < NS; sg++) {
-                ra[sg] = mk3(__shfl_sync(0xFFFFFFFFu, sa[sg].x, leader), __shfl_sync(0xFFFFFFFFu, sa[sg].y, leader),
-                             __shfl_sync(0xFFFFFFFFu, sa[sg].z, leader));
-                const float3 rd = mk3(__shfl_sync(0xFFFFFFFFu, sd[sg].x, leader),
-                                      __shfl_sync(0xFFFFFFFFu, sd[sg].y, leader),
-                                      __shfl_sync(0xFFFFFFFFu, sd[sg].z, leader));
-                const float3 rb = ra[sg] + rd;
-                rinv[sg] = inv_rd(rb - ra[sg]);
-                float dev = 0.0f, mag = 0.0f;
-                if (thr > 0.0f) {
-                    const float3 da = vabs(sa[sg] - ra[sg]), db = vabs((sa[sg] + sd[sg]) - rb);
-                    dev = fmaxf(fmaxf(fmaxf(da.x, da.y), da.z), fmaxf(fmaxf(db.x, db.y), db.z));
-                    const float3 ma = vabs(sa[sg]), mb = vabs(sa[sg] + sd[sg]);
-                    mag = fmaxf(fmaxf(fmaxf(ma.x, ma.y), ma.z), fmaxf(fmaxf(mb.x, mb.y), mb.z));
+                for (int i = 0; i < 2 * K; i++) xs[i] = e.x[i];
+            }
+            // the shadow segments of every root: endpoints are the chain's vertices and shading
+            // normals (contributableThroughput, pk.h:763-789), offset as occluded() does
+            float3 sa[NS], sd[NS];
+#pragma unroll
+            for (int sg = 0; sg < NS; sg++) sa[sg] = sd[sg] = mk3(0.f, 0.f, 0.f);
+            if (thr > 0.0f) {
+                float3 va, na;
+                chain_vertex<K>(ch, xs, S.p_light, pe, 0, va, na);
+#pragma unroll
+                for (int sg = 0; sg < NS; sg++) {
+                    float3 vb, nb, b;
+                    chain_vertex<K>(ch, xs, S.p_light, pe, sg + 1, vb, nb);
+                    shadow_segment(va, na, vb, nb, sa[sg], b);
+                    sd[sg] = ex::sub3(b, sa[sg]);
+                    va = vb;
+                    na = nb;
                 }
-                // covers the rounding of the slab and box arithmetic
-                rad[sg] = warp_max(dev) + 1.0e-5f * (1.0f + warp_max(mag));
             }
-            const int nc = fat_query_multi<NS>(S.nodes, root, ra, rinv, rad, (1u << NS) - 1u, cand[warp], front[warp]);
-            __syncwarp();
-            if (lane == 0) {
-                cQueries++;
-                if (nc < 0) cOverflow++;
-                else cCand += (unsigned long long)nc;
-            }
-            if (nc < 0) {
-                // the candidate list overflowed: each root walks the BVH itself
-                bool occ = false;
-                if (thr > 0.0f) {
+            const uint32_t valid = __ballot_sync(0xFFFFFFFFu, thr > 0.0f);
+            if (valid) {
+                // one merged query for all segments, each fattened to cover every root's segment
+                const int leader = __ffs(valid) - 1;
+                float3 ra[NS], rinv[NS];
+                float rad[NS];
+#pragma unroll
+                for (int sg = 0; sg < NS; sg++) {
+                    ra[sg] = mk3(__shfl_sync(0xFFFFFFFFu, sa[sg].x, leader), __shfl_sync(0xFFFFFFFFu, sa[sg].y, leader),
+                                 __shfl_sync(0xFFFFFFFFu, sa[sg].z, leader));
+                    const float3 rd = mk3(__shfl_sync(0xFFFFFFFFu, sd[sg].x, leader),
+                                          __shfl_sync(0xFFFFFFFFu, sd[sg].y, leader),
+                                          __shfl_sync(0xFFFFFFFFu, sd[sg].z, leader));
+                    const float3 rb = ra[sg] + rd;
+                    rinv[sg] = inv_rd(rb - ra[sg]);
+                    float dev = 0.0f, mag = 0.0f;
+                    if (thr > 0.0f) {
+                        const float3 da = vabs(sa[sg] - ra[sg]), db = vabs((sa[sg] + sd[sg]) - rb);
+                        dev = fmaxf(fmaxf(fmaxf(da.x, da.y), da.z), fmaxf(fmaxf(db.x, db.y), db.z));
+                        const float3 ma = vabs(sa[sg]), mb = vabs(sa[sg] + sd[sg]);
+                        mag = fmaxf(fmaxf(fmaxf(ma.x, ma.y), ma.z), fmaxf(fmaxf(mb.x, mb.y), mb.z));
+                    }
+                    // covers the rounding of the slab and box arithmetic
+                    rad[sg] = warp_max(dev) + 1.0e-5f * (1.0f + warp_max(mag));
+                }
+                const int nc = fat_query_multi<NS>(S.nodes, root, ra, rinv, rad, (1u << NS) - 1u, cand[warp], front[warp]);
+                __syncwarp();
+                if (lane == 0) {
+                    cQueries++;
+                    if (nc < 0) cOverflow++;
+                    else cCand += (unsigned long long)nc;
+                }
+                if (nc < 0) {
+                    // the candidate list overflowed: each root walks the BVH itself
+                    bool occ = false;
+                    if (thr > 0.0f) {
 #pragma unroll 1
-                    for (int sg = 0; sg < NS && !occ; sg++)
-                        occ = any_hit(S.nodes, S.tris, root, pick3<NS>(sa, sg), pick3<NS>(sd, sg), 1.0f) < 1.0f;
-                }
-                if (occ) thr = 0.0f;
-            } else if (nc > 0) {
-                // The nc x nv (candidate, root) tests are spread over all 32 lanes, candidate
-                // major (neighbouring lanes load the same triangle), instead of each root's lane
-                // testing every candidate while the lanes without a root idle.  A root is
-                // occluded when any of its tests hits before the segment's end; tests of roots
-                // already found occluded are skipped.
-                if (thr > 0.0f) {
+                        for (int sg = 0; sg < NS && !occ; sg++)
+                            occ = any_hit(S.nodes, S.tris, root, pick3<NS>(sa, sg), pick3<NS>(sd, sg), 1.0f) < 1.0f;
+                    }
+                    if (occ) thr = 0.0f;
+                } else if (nc > 0) {
+                    // The nc x nv (candidate, root) tests are spread over all 32 lanes, candidate
+                    // major (neighbouring lanes load the same triangle), instead of each root's lane
+                    // testing every candidate while the lanes without a root idle.  A root is
+                    // occluded when any of its tests hits before the segment's end; tests of roots
+                    // already found occluded are skipped.
+                    if (thr > 0.0f) {
 #pragma unroll
-                    for (int sg = 0; sg < NS; sg++) {
-                        segA[warp][sg][0][lane] = sa[sg].x;
-                        segA[warp][sg][1][lane] = sa[sg].y;
-                        segA[warp][sg][2][lane] = sa[sg].z;
-                        segD[warp][sg][0][lane] = sd[sg].x;
-                        segD[warp][sg][1][lane] = sd[sg].y;
-                        segD[warp][sg][2][lane] = sd[sg].z;
+                        for (int sg = 0; sg < NS; sg++) {
+                            segA[warp][sg][0][lane] = sa[sg].x;
+                            segA[warp][sg][1][lane] = sa[sg].y;
+                            segA[warp][sg][2][lane] = sa[sg].z;
+                            segD[warp][sg][0][lane] = sd[sg].x;
+                            segD[warp][sg][1][lane] = sd[sg].y;
+                            segD[warp][sg][2][lane] = sd[sg].z;
+                        }
                     }
+                    if (lane == 0) occMask[warp] = 0u;
+                    __syncwarp();
+                    const int nv = __popc(valid);
+                    const int total = nc * nv;
+                    const int dq = 32 / nv, dr = 32 % nv;
+                    int c = lane / nv, rr = lane % nv;
+                    volatile uint32_t* occ = &occMask[warp];
+                    for (int pIdx = lane; pIdx < total; pIdx += 32) {
+                        const int src = (int)__fns(valid, 0, rr + 1);
+                        if (!((*occ >> src) & 1u)) {
+                            const uint32_t e = cand[warp][c];
+                            const uint32_t sg = e >> kSegShift;
+                            float3 v0, v1, v2;
+                            load_tri(S.tris, e & kIdxMask, v0, v1, v2);
+                            float t, u, v;
+                            float3 ng;
+                            const float3 ro = mk3(segA[warp][sg][0][src], segA[warp][sg][1][src], segA[warp][sg][2][src]);
+                            const float3 rd = mk3(segD[warp][sg][0][src], segD[warp][sg][1][src], segD[warp][sg][2][src]);
+                            if (ray_triangle(&t, &u, &v, &ng, 0.0f, 1.0f, ro, rd, v0, v1, v2) &&
+                                t < 1.0f)
+                                atomicOr(&occMask[warp], 1u << src);
+                        }
+                        c += dq;
+                        rr += dr;
+                        if (rr >= nv) {
+                            rr -= nv;
+                            c++;
+                        }
+                    }
+                    __syncwarp();
+                    if ((occMask[warp] >> lane) & 1u) thr = 0.0f;
                 }
-                if (lane == 0) occMask[warp] = 0u;
                 __syncwarp();
-                const int nv = __popc(valid);
-                const int total = nc * nv;
-                const int dq = 32 / nv, dr = 32 % nv;
-                int c = lane / nv, rr = lane % nv;
-                volatile uint32_t* occ = &occMask[warp];
-                for (int pIdx = lane; pIdx < total; pIdx += 32) {
-                    const int src = (int)__fns(valid, 0, rr + 1);
-                    if (!((*occ >> src) & 1u)) {
-                        const uint32_t e = cand[warp][c];
-                        const uint32_t sg = e >> kSegShift;
-                        float3 v0, v1, v2;
-                        load_tri(S.tris, e & kIdxMask, v0, v1, v2);
-                        float t, u, v;
-                        float3 ng;
-                        const float3 ro = mk3(segA[warp][sg][0][src], segA[warp][sg][1][src], segA[warp][sg][2][src]);
-                        const float3 rd = mk3(segD[warp][sg][0][src], segD[warp][sg][1][src], segD[warp][sg][2][src]);
-                        if (ray_triangle(&t, &u, &v, &ng, 0.0f, 1.0f, ro, rd, v0, v1, v2) &&
-                            t < 1.0f)
-                            atomicOr(&occMask[warp], 1u << src);
-                    }
-                    c += dq;
-                    rr += dr;
-                    if (rr >= nv) {
-                        rr -= nv;
-                        c++;
-                    }
-                }
-                __syncwarp();
-                if ((occMask[warp] >> lane) & 1u) thr = 0.0f;
             }
-            __syncwarp();
+            if (mine && !(thr > 0.0f)) acc[blk.first + idx].thr = 0.0f;
         }
-        if (mine && !(thr > 0.0f)) acc[blk.first + lane].thr = 0.0f;
     }
     if (a.counters) {
         flush_count(a.counters + kCntQueries, cQueries);
