@@ -310,9 +310,9 @@ PZ_API int pz_solve_constraints(int K, uint32_t events, pz_float3 p_beg, const i
  * (e.g. its lookup counter; NULL entries or a NULL array: descs[i].n_paths), descs[i].n_paths
  * its capacity.  pz_solve_specular_multi then only enqueues work (memsets and kernels), so
  * a frame that calls it can be captured in a CUDA graph.  Tuning: probe / phase-1 blocks per
- * SM, phase-2 blocks per SM (1 or 2), and p2_chunk, which must be 1 (phase 2 takes one
- * record per queue access); NULL = the best found by pz_solve_multi_autotune for this (K,
- * bins, capacity), else {8, 2, 1}.
+ * SM, phase-2 blocks per SM (1 or 2), and records a phase-2 warp claims per queue access
+ * (1..8); NULL = the best found by pz_solve_multi_autotune for this (K, bins, capacity),
+ * else {8, 2, 4}.
  * pz_solve_multi_autotune renders the batch once per candidate (clear the images after
  * it) and keeps the fastest. */
 typedef struct pz_batch_tuning { int p1_blocks_per_sm, p2_blocks_per_sm, p2_chunk; } pz_batch_tuning;

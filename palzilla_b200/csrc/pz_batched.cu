@@ -733,9 +733,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kP2SolveBlocks) k_p2_solv
     unsigned long long* const nBlocks = a.p2 + 1;
     unsigned long long* const reserved = a.p2 + 2;
     unsigned long long nConv = 0, cNewton = 0, cPolish = 0, cIters = 0, cWarm = 0;
-    // The warp's current record and the bins of it not yet handed to a lane (warp-uniform).
-    unsigned long long jc = 0, mc = 0;
+    // The warp's current record and the bins of it not yet handed to a lane, and the records
+    // it has claimed and not yet started, [jNext, jEnd) (all warp-uniform).
+    unsigned long long jc = 0, mc = 0, jNext = 0, jEnd = 0;
     bool drained = false;
+    const unsigned long long chunk = (unsigned long long)(a.chunk > 0 ? a.chunk : kP2ChunkDefault);
     // accepted roots held back for the next round: ns entries of record stashRec
     __shared__ Accepted<K> stash[kWarpsPerBlock][32];
     const int warp = threadIdx.x >> 5;
@@ -746,33 +748,37 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kP2SolveBlocks) k_p2_solv
         // from the photon's start) starts a round, or joins one only if all its bins fit, so
         // the bins of a round mostly share one chain and one start and follow similar Newton
         // paths.  A predicted record is packed: its bins in rank order, then the next
-        // record's, so no lane idles for a bin that a record's mask excludes.  A record is
-        // taken after reserving room for B accepted roots (a record never has more) in this
-        // wave.
+        // record's, so no lane idles for a bin that a record's mask excludes.  Records are
+        // claimed `chunk` at a time (one atomic each on the work counter and on the room
+        // reserved for B accepted roots per record, a record's most, in this wave).
         int filled = 0;
         unsigned long long myRec = 0;
         int myBin = -1;
         while (filled < 32) {
             if (mc == 0) {
-                if (drained) break;
-                unsigned long long j = 0;
-                bool take = false;
-                if (lane == 0) {
-                    if (*a.workCounter < nRec && atomicAdd(reserved, (unsigned long long)B) + (unsigned long long)B <= a.acceptCapacity) {
-                        j = atomicAdd(a.workCounter, 1ull);
-                        take = j < nRec;
+                if (jNext == jEnd) {
+                    if (drained) break;
+                    unsigned long long j = 0, cnt = 0;
+                    if (lane == 0) {
+                        const unsigned long long room = (unsigned long long)B * chunk;
+                        if (*a.workCounter < nRec && atomicAdd(reserved, room) + room <= a.acceptCapacity) {
+                            j = atomicAdd(a.workCounter, chunk);
+                            cnt = j < nRec ? min(chunk, nRec - j) : 0ull;
+                        }
                     }
+                    cnt = __shfl_sync(0xFFFFFFFFu, cnt, 0);
+                    if (cnt == 0) {
+                        drained = true;
+                        break;
+                    }
+                    jNext = __shfl_sync(0xFFFFFFFFu, j, 0);
+                    jEnd = jNext + cnt;
                 }
-                take = __shfl_sync(0xFFFFFFFFu, take, 0);
-                if (!take) {
-                    drained = true;
-                    break;
-                }
-                j = __shfl_sync(0xFFFFFFFFu, j, 0);
-                const bool whole = j < nRec2;
-                jc = whole ? a.recordCapacity - 1 - j : j - nRec2;
-                mc = record_todo<K>(recs[jc], B);
+                const bool whole = jNext < nRec2;
                 if (whole && filled != 0 && B > 32 - filled) break;  // it starts the next round
+                jc = whole ? a.recordCapacity - 1 - jNext : jNext - nRec2;
+                jNext++;
+                mc = record_todo<K>(recs[jc], B);
                 continue;
             }
             const int n = min(__popcll(mc), 32 - filled);

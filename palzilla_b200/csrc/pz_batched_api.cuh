@@ -26,7 +26,7 @@ struct BatchArgs {
     float grazeCos = 0.0f;             // FP64 polish and admissibility below this |cos| (<= 0: never)
     int continuation;                  // 1: refine predicted roots instead of solving from the photon start
     float illDet;                      // relative det below which an item takes per-bin solves (near a fold)
-    int chunk = 0;                     // records a phase-2 warp takes per queue access (0: 1)
+    int chunk = 0;                     // records a phase-2 warp claims per queue access (0: kP2ChunkDefault)
     const SceneArgs* scenes = nullptr; // batch of scenes (device table), or null: the single scene s
     uint32_t nScenes = 0;
     const unsigned long long* offsets = nullptr;  // nScenes + 1 item offsets of the batch
@@ -55,15 +55,28 @@ constexpr int kPhase1Blocks = PZ_PHASE1_BLOCKS;
 // Relative determinant of an item's branch of roots below which the item is solved bin by bin
 // (near a fold of the caustic, where the prediction of the bins' roots is least reliable).
 constexpr float kDefaultFoldDet = 1.0e-2f;
+// Phase-2 warps claim records in chunks of up to kP2ChunkMax (kP2ChunkDefault unless a tuning
+// says otherwise); a wave's room is padded by one chunk so that it still takes its share of
+// the records when its last reservations are for whole chunks.
+#ifndef PZ_P2_CHUNK
+#define PZ_P2_CHUNK 4
+#endif
+constexpr int kP2ChunkMax = 8;
+constexpr int kP2ChunkDefault = PZ_P2_CHUNK;
+static_assert(kP2ChunkDefault >= 1 && kP2ChunkDefault <= kP2ChunkMax, "PZ_P2_CHUNK: 1..8");
+inline unsigned long long wave_records(unsigned long long recordCapacity)
+{
+    return (recordCapacity + kMaxWaves - 1) / kMaxWaves + kP2ChunkMax;
+}
 inline unsigned long long accept_capacity(unsigned long long recordCapacity, int nBins)
 {
-    return (unsigned long long)nBins * ((recordCapacity + kMaxWaves - 1) / kMaxWaves);
+    return (unsigned long long)nBins * wave_records(recordCapacity);
 }
 // at most three rounds (blocks) per record: B <= 64 bins on consecutive lanes of 32-lane
 // rounds that other records' bins may start and end
 inline unsigned long long block_capacity(unsigned long long recordCapacity)
 {
-    return 3ull * ((recordCapacity + kMaxWaves - 1) / kMaxWaves);
+    return 3ull * wave_records(recordCapacity);
 }
 
 // One scene of a batch: its solve arguments and its item count on the device.

@@ -446,7 +446,7 @@ extern "C" int pz_solve_specular_multi(int K, int n_bins, uint32_t n_scenes, uin
     int r = multi_args(K, n_bins, n_scenes, max_paths_total, scratch_dev, scratch_bytes, stats_dev, &b, &offsets,
                        "pz_solve_specular_multi");
     if (r != PZ_OK) return r;
-    pz_batch_tuning t = {8, 2, 1};
+    pz_batch_tuning t = {8, 2, batched::kP2ChunkDefault};
     if (tuning) {
         t = *tuning;
     } else {
@@ -455,7 +455,7 @@ extern "C" int pz_solve_specular_multi(int K, int n_bins, uint32_t n_scenes, uin
         if (it != g_tunings.end()) t = it->second;
     }
     if (t.p1_blocks_per_sm < 1 || t.p1_blocks_per_sm > 32 || t.p2_blocks_per_sm < 1 || t.p2_blocks_per_sm > 2 ||
-        t.p2_chunk != 1)
+        t.p2_chunk < 1 || t.p2_chunk > batched::kP2ChunkMax)
         return fail(PZ_ERR_INVALID_ARGUMENT, "pz_solve_specular_multi: tuning out of range");
     return done(run_multi(K, b, t, offsets, scratch_dev, S(stream)), "pz_solve_specular_multi");
 }
@@ -476,7 +476,7 @@ extern "C" int pz_solve_multi_autotune(int K, int n_bins, uint32_t n_scenes, uin
     pz_batch_tuning best = {8, 2, 1};
     float bestMs = 3.4e38f;
     cudaError_t e = run_multi(K, b, best, offsets, scratch_dev, s);  // warm-up
-    const int p1s[] = {4, 8, 16}, p2s[] = {1, 2}, chunks[] = {1};
+    const int p1s[] = {4, 8, 16}, p2s[] = {1, 2}, chunks[] = {1, 4};
     for (int p1 : p1s)
         for (int p2 : p2s)
             for (int c : chunks) {
