@@ -54,9 +54,9 @@ LAUNCHES_PER_FRAME = 12 + 8 * 3
 # Per work item of the batched solve stage (k_probe, k_phase1 and the 8 phase-2 waves of
 # k_p2_solve / k_p2_vis / k_p2_contrib), from one ncu capture of every launch of one frame
 # of this workload at 256x256 (1,256,661 work items; summarised under profiles/):
-# DRAM bytes read + written (1007.6 MB) and warp instructions issued (4.681 G).
-NCU_SOLVE_DRAM_PER_ITEM = 801.8
-NCU_SOLVE_WARP_INST_PER_ITEM = 3725.0
+# DRAM bytes read + written (1046.5 MB) and warp instructions issued (4.640 G).
+NCU_SOLVE_DRAM_PER_ITEM = 832.7
+NCU_SOLVE_WARP_INST_PER_ITEM = 3692.0
 ISSUE_PER_SM_PER_CLOCK = 4  # one warp instruction per cycle on each of an SM's 4 schedulers
 
 
