@@ -920,6 +920,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kP2SolveBlocks) k_p2_solv
     }
 }
 
+#ifndef PZ_VIS_GROUP
+#define PZ_VIS_GROUP 2
+#endif
+constexpr unsigned long long kVisGroup = PZ_VIS_GROUP;  // blocks a visibility warp claims at once (even)
+static_assert(PZ_VIS_GROUP >= 2 && PZ_VIS_GROUP % 2 == 0, "PZ_VIS_GROUP: an even count");
+
 template <int K, bool kMulti>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, 3) k_p2_vis(BatchArgs a)
 {
@@ -945,10 +951,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 3) k_p2_vis(BatchArgs a)
         // Blocks are taken in pairs.  Two blocks of one tuple (consecutive records: the work
         // list is in tuple order, so neighbouring pixels) whose roots fit the warp share one
         // query, fattened to cover both; otherwise the warp runs them one after the other.
-        unsigned long long bi = 0;
-        if (lane == 0) bi = atomicAdd(a.p2 + 3, 2ull);
-        bi = __shfl_sync(0xFFFFFFFFu, bi, 0);
-        if (bi >= nB) break;
+        unsigned long long bg = 0;
+        if (lane == 0) bg = atomicAdd(a.p2 + 3, (unsigned long long)kVisGroup);
+        bg = __shfl_sync(0xFFFFFFFFu, bg, 0);
+        if (bg >= nB) break;
+        for (unsigned long long bi = bg; bi < bg + kVisGroup && bi < nB; bi += 2) {
         const AcceptBlock b0 = blocks[bi];
         const bool has1 = bi + 1 < nB;
         const AcceptBlock b1 = has1 ? blocks[bi + 1] : AcceptBlock{0u, b0.rec, 0u};
@@ -1095,6 +1102,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 3) k_p2_vis(BatchArgs a)
                 __syncwarp();
             }
             if (mine && !(thr > 0.0f)) acc[blk.first + idx].thr = 0.0f;
+        }
         }
     }
     if (a.counters) {
