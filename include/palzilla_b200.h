@@ -142,8 +142,9 @@ PZ_API int pz_trace_any(const pz_internal_node* internals_dev, const uint32_t* r
 
 /* ---------------------------------------------------------------- PathCache
  * Spatial hash of photon tuples (PathCache, pk.h:227-402) in one caller-owned buffer of
- * pz_path_cache_bytes(capacity) bytes; capacity must be a power of two (the reference
- * uses 2^22).  The status word (first 4 bytes) reports probe overflow. */
+ * pz_path_cache_bytes(capacity) bytes starting on a 16-byte boundary; capacity must be a
+ * power of two (the reference uses 2^22).  The status word (first 4 bytes) reports probe
+ * overflow. */
 PZ_API size_t pz_path_cache_bytes(uint32_t capacity);
 /* PathCache::clear (pk.h:254-269): empties the table and the counters. */
 PZ_API int pz_path_cache_clear(void* cache_dev, uint32_t capacity, pz_stream_t stream);

@@ -74,45 +74,49 @@ PZ_D uint32_t spacial_hash(float3 p, float step)
     return hash_of_iP(__float2int_rz(floorf(idx.x)), __float2int_rz(floorf(idx.y)), __float2int_rz(floorf(idx.z)));
 }
 
-// PathCache::store, pk.h:291-349
-PZ_D bool cache_store(const CacheView& c, float3 pos, const int* tris, const float* params, uint32_t ev)
+// The hash of the k-th (0..7) of the 8 cells nearest to pos, in the reference's order
+// (x fastest, then y, then z; pk.h:303-311).
+PZ_D uint32_t cache_cell_hash(const CacheView& c, float3 pos, int k)
 {
-    const uint32_t hp = path_hash(ev, tris);
-    const int K = (int)(ev >> 24);
+    const float3 idx = pos / c.step;
+    const int x = __float2int_rz(floorf(idx.x)), y = __float2int_rz(floorf(idx.y)), z = __float2int_rz(floorf(idx.z));
+    const int dx = idx.x - (float)x < 0.5f ? -1 : 1;
+    const int dy = idx.y - (float)y < 0.5f ? -1 : 1;
+    const int dz = idx.z - (float)z < 0.5f ? -1 : 1;
+    return hash_of_iP(x + (k & 1) * dx, y + ((k >> 1) & 1) * dy, z + (k >> 2) * dz);
+}
+
+// One cell of PathCache::store (pk.h:312-345): the probe from the cell hash's home slot.
+// It visits the same slots in the same order and stops on the same conditions as the
+// reference's CAS-per-slot loop, but reads each slot from L2 first (atomics live there):
+// a slot holding this path hash ends the probe, one holding another hash is passed, and
+// only a slot that reads empty is claimed with the CAS, whose answer is then handled
+// like the reference's.  Slots go from empty to a path hash once and never change while
+// photons are stored, so a read that saw a hash sees what the CAS would have returned.
+// t and p0/p1 are the tuple's triangle indices and barycentrics, zero past its length.
+PZ_D void cache_store_cell(const CacheView& c, uint32_t hP, uint32_t hp, uint32_t ev, int4 t, float4 p0, float4 p1)
+{
     const uint32_t mask = c.capacity - 1u;
-    bool success = false;
-    float3 idx = pos / c.step;
-    int x = __float2int_rz(floorf(idx.x)), y = __float2int_rz(floorf(idx.y)), z = __float2int_rz(floorf(idx.z));
-    int dx = idx.x - (float)x < 0.5f ? -1 : 1;
-    int dy = idx.y - (float)y < 0.5f ? -1 : 1;
-    int dz = idx.z - (float)z < 0.5f ? -1 : 1;
-    for (int iz = 0; iz < 2; iz++)
-        for (int iy = 0; iy < 2; iy++)
-            for (int ix = 0; ix < 2; ix++) {
-                const uint32_t hP = hash_of_iP(x + ix * dx, y + iy * dy, z + iz * dz);
-                const uint32_t home = hP & mask;
-                uint32_t off = 0;
-                for (; off < kMaxProbe; off++) {
-                    const uint32_t i = (home + off) & mask;
-                    const uint32_t old = atomicCAS(c.hash + i, 0u, hp);
-                    if (old == 0u) {
-                        c.cell[i] = hP;
-                        c.event[i] = ev;
-                        c.tris[i] = make_int4(tris[0], K > 1 ? tris[1] : 0, K > 2 ? tris[2] : 0, K > 3 ? tris[3] : 0);
-                        float p[8];
-                        for (int d = 0; d < 8; d++) p[d] = d < 2 * K ? params[d] : 0.0f;
-                        c.params[2 * i] = make_float4(p[0], p[1], p[2], p[3]);
-                        c.params[2 * i + 1] = make_float4(p[4], p[5], p[6], p[7]);
-                        success = true;
-                        atomicAdd(&c.h->count, 1u);
-                        break;
-                    } else if (old == hp) {
-                        break;
-                    }
-                }
-                if (off == kMaxProbe) raise_error(&c.h->status, kErrCapacity);
-            }
-    return success;
+    const uint32_t home = hP & mask;
+    uint32_t off = 0;
+    for (; off < kMaxProbe; off++) {
+        const uint32_t i = (home + off) & mask;
+        const uint32_t seen = __ldcg(c.hash + i);
+        if (seen == hp) break;
+        if (seen != 0u) continue;
+        const uint32_t old = atomicCAS(c.hash + i, 0u, hp);
+        if (old == 0u) {
+            c.cell[i] = hP;
+            c.event[i] = ev;
+            c.tris[i] = t;
+            c.params[2 * i] = p0;
+            c.params[2 * i + 1] = p1;
+            atomicAdd(&c.h->count, 1u);
+            break;
+        }
+        if (old == hp) break;
+    }
+    if (off == kMaxProbe) raise_error(&c.h->status, kErrCapacity);
 }
 
 }  // namespace pz

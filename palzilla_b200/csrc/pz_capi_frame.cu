@@ -57,9 +57,15 @@ extern "C" int pz_trace_any(const pz_internal_node* internals_dev, const uint32_
 // ---------------------------------------------------------------- PathCache
 extern "C" size_t pz_path_cache_bytes(uint32_t capacity) { return pow2(capacity) ? cache_bytes(capacity) : 0; }
 
+// the store writes each slot's triangle indices and barycentrics as 16-byte vectors
+static bool cache_ok(const void* cache_dev, uint32_t capacity)
+{
+    return cache_dev && (reinterpret_cast<uintptr_t>(cache_dev) & 15u) == 0 && pow2(capacity);
+}
+
 extern "C" int pz_path_cache_clear(void* cache_dev, uint32_t capacity, pz_stream_t stream)
 {
-    if (!cache_dev || !pow2(capacity)) return fail(PZ_ERR_INVALID_ARGUMENT, "pz_path_cache_clear: bad argument");
+    if (!cache_ok(cache_dev, capacity)) return fail(PZ_ERR_INVALID_ARGUMENT, "pz_path_cache_clear: bad argument");
     CacheView c = cache_view(cache_dev, capacity, 0.0f);
     cudaError_t e = cudaMemsetAsync(c.h, 0, sizeof(CacheHeader), S(stream));
     if (e == cudaSuccess) e = cudaMemsetAsync(c.hash, 0, sizeof(uint32_t) * (size_t)capacity, S(stream));
@@ -69,7 +75,7 @@ extern "C" int pz_path_cache_clear(void* cache_dev, uint32_t capacity, pz_stream
 extern "C" int pz_path_cache_views(void* cache_dev, uint32_t capacity, uint32_t** hash_dev, uint32_t** cell_dev,
                                    uint32_t** events_dev, int32_t** tris_dev, float** params_dev, uint32_t** count_dev)
 {
-    if (!cache_dev || !pow2(capacity)) return fail(PZ_ERR_INVALID_ARGUMENT, "pz_path_cache_views: bad argument");
+    if (!cache_ok(cache_dev, capacity)) return fail(PZ_ERR_INVALID_ARGUMENT, "pz_path_cache_views: bad argument");
     CacheView c = cache_view(cache_dev, capacity, 0.0f);
     if (hash_dev) *hash_dev = c.hash;
     if (cell_dev) *cell_dev = c.cell;
@@ -90,8 +96,9 @@ extern "C" int pz_photon_trace(const pz_internal_node* internals_dev, const uint
 {
     if (n_triangles < 0 || photons_per_triangle < 0 || !root_dev || (n_triangles > 0 && (!triangles_dev || !attribs_dev)))
         return fail(PZ_ERR_INVALID_ARGUMENT, "pz_photon_trace: bad argument");
-    if (cache_dev && (!pow2(cache_capacity) || !(cell_step > 0.0f)))
-        return fail(PZ_ERR_INVALID_ARGUMENT, "pz_photon_trace: cache capacity must be a power of two, step > 0");
+    if (cache_dev && (!cache_ok(cache_dev, cache_capacity) || !(cell_step > 0.0f)))
+        return fail(PZ_ERR_INVALID_ARGUMENT,
+                    "pz_photon_trace: cache must be 16-byte aligned, capacity a power of two, step > 0");
     CacheView c{};
     if (cache_dev) c = cache_view(cache_dev, cache_capacity, cell_step);
     return done(launch_photons(reinterpret_cast<const Node*>(internals_dev), root_dev,
@@ -160,8 +167,8 @@ extern "C" int pz_lookup_flatten(uint32_t events, pz_specular_path* paths_dev, u
                                  int n_pixels, void* cache_dev, uint32_t cache_capacity, float cell_step,
                                  pz_stream_t stream)
 {
-    if (n_pixels < 0 || !paths_dev || !indexed_dev || !counter_dev || !first_diffuse_dev || !cache_dev ||
-        !pow2(cache_capacity) || !(cell_step > 0.0f))
+    if (n_pixels < 0 || !paths_dev || !indexed_dev || !counter_dev || !first_diffuse_dev ||
+        !cache_ok(cache_dev, cache_capacity) || !(cell_step > 0.0f))
         return fail(PZ_ERR_INVALID_ARGUMENT, "pz_lookup_flatten: bad argument");
     return done(launch_lookup(events, reinterpret_cast<SpecularPath*>(paths_dev),
                               reinterpret_cast<unsigned long long*>(indexed_dev), counter_dev, capacity,
@@ -189,7 +196,7 @@ int solve_args_from_desc(const pz_solve_desc* d, SolveArgs* a, const char* who)
     if (d->K < 1 || d->K > 4) return fail(PZ_ERR_INVALID_ARGUMENT, "%s: K must be 1..4 (got %d)", who, d->K);
     if ((int)(d->events >> 24) != d->K)
         return fail(PZ_ERR_INVALID_ARGUMENT, "%s: event descriptor size %u != K %d", who, d->events >> 24, d->K);
-    if (!d->cache || !pow2(d->cache_capacity) || !(d->cell_step > 0.0f))
+    if (!cache_ok(d->cache, d->cache_capacity) || !(d->cell_step > 0.0f))
         return fail(PZ_ERR_INVALID_ARGUMENT, "%s: bad cache", who);
     if (d->n_paths && (!d->paths || !d->first_diffuse || !d->root || !d->triangles || !d->attribs))
         return fail(PZ_ERR_INVALID_ARGUMENT, "%s: null buffer", who);

@@ -10,6 +10,12 @@
 // n_triangles x photons_per_triangle photons (the reference's 256-thread block per
 // triangle is the photons_per_triangle = 256 case).  Diffuse and back-facing
 // emitters retire at once, as in the reference.
+//
+// PathCache stores (PathCache::store, pk.h:291-349) are made by the whole warp at the
+// end: each landed photon's 8 cell probes are spread over the warp's lanes, the photon's
+// tuple passed through shared memory, so a warp with few landings does not run 8 probes
+// in a row on one lane.  Which photon's barycentrics fill a new slot is decided by the
+// CAS race, as in the reference.
 #include "pz_cache.cuh"
 #include "pz_optics.cuh"
 #include "pz_photon.cuh"
@@ -18,12 +24,13 @@
 namespace pz {
 
 constexpr int kPhotonDepth = 4;  // PHOTON_TRACE_MAX_DEPTH, pk.h:33
+constexpr int kPhotonBlock = 256;
 
 #ifndef PZ_PHOTON_MIN_BLOCKS
 #define PZ_PHOTON_MIN_BLOCKS 1
 #endif
 
-__global__ void __launch_bounds__(256, PZ_PHOTON_MIN_BLOCKS) k_photon(const Node* __restrict__ nodes, const uint32_t* __restrict__ rootPtr,
+__global__ void __launch_bounds__(kPhotonBlock, PZ_PHOTON_MIN_BLOCKS) k_photon(const Node* __restrict__ nodes, const uint32_t* __restrict__ rootPtr,
                                                 const Tri* __restrict__ tris, const Attrib* __restrict__ attribs,
                                                 uint32_t nTris, uint32_t photonsPerTri, float3 p_light, float eta_min,
                                                 float eta_max, int iteration, float minThroughput, CacheView cache,
@@ -32,13 +39,18 @@ __global__ void __launch_bounds__(256, PZ_PHOTON_MIN_BLOCKS) k_photon(const Node
     const uint64_t gid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t iTri = (uint32_t)(gid / photonsPerTri);
     const uint32_t j = (uint32_t)(gid % photonsPerTri);
-    if (iTri >= nTris) return;
+    const bool live = iTri < nTris;  // every lane reaches the warp's stores below
+    bool landed = false;
+    float3 p_land = mk3(0.f, 0.f, 0.f);
+    uint32_t ev_land = 0;
+    int4 t_land = make_int4(0, 0, 0, 0);
+    float4 b0 = make_float4(0.f, 0.f, 0.f, 0.f), b1 = b0;
     PhotonRecord rec;
     rec.ev = 0;
     bool emitted = false;
     const uint32_t root = __ldg(rootPtr);
 
-    const int32_t mat0 = __ldg(&attribs[iTri].material);
+    const int32_t mat0 = live ? __ldg(&attribs[iTri].material) : kDiffuse;
     if (mat0 != kDiffuse) {
         float3 v0, v1, v2;
         load_tri(tris, iTri, v0, v1, v2);
@@ -112,7 +124,16 @@ __global__ void __launch_bounds__(256, PZ_PHOTON_MIN_BLOCKS) k_photon(const Node
             if (admissible && minThroughput < throughput) {
                 ev |= (uint32_t)K << 24;
                 emitted = true;
-                if (cache.hash) cache_store(cache, p_final, triIdx, params, ev);
+                if (cache.hash) {
+                    landed = true;
+                    p_land = p_final;
+                    ev_land = ev;
+                    t_land = make_int4(triIdx[0], K > 1 ? triIdx[1] : 0, K > 2 ? triIdx[2] : 0, K > 3 ? triIdx[3] : 0);
+                    float q[8];
+                    for (int d = 0; d < 8; d++) q[d] = d < 2 * K ? params[d] : 0.0f;
+                    b0 = make_float4(q[0], q[1], q[2], q[3]);
+                    b1 = make_float4(q[4], q[5], q[6], q[7]);
+                }
                 if (records) {
                     rec.ev = ev;
                     for (int d = 0; d < 4; d++) rec.tris[d] = triIdx[d];
@@ -124,6 +145,34 @@ __global__ void __launch_bounds__(256, PZ_PHOTON_MIN_BLOCKS) k_photon(const Node
             }
         }
     }
+    // the warp's landed photons, packed to the front of the warp's shared slots: landing
+    // point with the path hash in w, event descriptor, triangles, barycentrics
+    __shared__ float4 shPos[kPhotonBlock];
+    __shared__ uint32_t shEv[kPhotonBlock];
+    __shared__ int4 shTris[kPhotonBlock];
+    __shared__ float4 shBary[2 * kPhotonBlock];
+    __syncwarp();
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t landMask = __ballot_sync(0xffffffffu, landed);
+    const int nLand = __popc(landMask);
+    const int warpBase = (int)(threadIdx.x & ~31u);
+    if (landed) {
+        const int r = warpBase + __popc(landMask & ((1u << lane) - 1u));
+        const int tl[4] = {t_land.x, t_land.y, t_land.z, t_land.w};
+        shPos[r] = make_float4(p_land.x, p_land.y, p_land.z, __uint_as_float(path_hash(ev_land, tl)));
+        shEv[r] = ev_land;
+        shTris[r] = t_land;
+        shBary[2 * r] = b0;
+        shBary[2 * r + 1] = b1;
+    }
+    __syncwarp();
+    for (int task = (int)lane; task < 8 * nLand; task += 32) {
+        const int src = warpBase + (task >> 3);
+        const float4 pw = shPos[src];
+        const uint32_t hP = cache_cell_hash(cache, mk3(pw.x, pw.y, pw.z), task & 7);
+        cache_store_cell(cache, hP, __float_as_uint(pw.w), shEv[src], shTris[src], shBary[2 * src], shBary[2 * src + 1]);
+    }
+    if (!live) return;
     if (records) {
         if (!emitted) {
             for (int d = 0; d < 4; d++) rec.tris[d] = 0;
@@ -142,7 +191,7 @@ cudaError_t launch_photons(const Node* nodes, const uint32_t* root, const Tri* t
     const uint64_t total = (uint64_t)nTris * photonsPerTri;
     if (total == 0) return cudaSuccess;
     const uint64_t blocks = (total + 255) / 256;
-    k_photon<<<(unsigned)blocks, 256, 0, s>>>(nodes, root, tris, attribs, nTris, photonsPerTri, p_light, eta_min,
+    k_photon<<<(unsigned)blocks, kPhotonBlock, 0, s>>>(nodes, root, tris, attribs, nTris, photonsPerTri, p_light, eta_min,
                                               eta_max, iteration, minThroughput, cache, records);
     return cudaGetLastError();
 }

@@ -44,3 +44,13 @@ def test_host_side_argument_checks():
     r = L.pz_bvh_build(None, -1, 0, None, None, None, C.c_size_t(0), None)
     assert r == 1
     assert L.pz_onesweep_scratch_bytes(1 << 20) > 0
+    # the PathCache buffer starts on a 16-byte boundary with a power-of-two capacity; the
+    # views call only computes addresses, so a made-up device address is enough here
+    hp = C.c_void_p()
+    r = L.pz_path_cache_views(C.c_void_p(0x10000), C.c_uint32(1 << 10), C.byref(hp), None, None, None, None, None)
+    assert r == 0 and hp.value == 0x10000 + 256 + 48 * (1 << 10)
+    r = L.pz_path_cache_views(C.c_void_p(0x10004), C.c_uint32(1 << 10), None, None, None, None, None, None)
+    assert r == 1 and b"pz_path_cache_views" in L.pz_last_error()
+    r = L.pz_path_cache_views(C.c_void_p(0x10000), C.c_uint32(3), None, None, None, None, None, None)
+    assert r == 1
+    assert L.pz_path_cache_bytes(C.c_uint32(3)) == 0 and L.pz_path_cache_bytes(C.c_uint32(4)) > 0

@@ -113,6 +113,31 @@ def test_path_cache_contents(orc, lens, lens_bvh):
                    np.array_equal(c["params"], g["params"][i]) for c in cands)
 
 
+@pytest.mark.parametrize("capacity", [1, 2, 4, 16, 1 << 16])
+def test_path_cache_small_tables(orc, lens, lens_bvh, capacity):
+    """Tables below four slots probe one slot at a time; full tables stop each probe after
+    the probe limit with the capacity bit, holding only paths the photons carried."""
+    sc, ds = lens
+    ppt = 2
+    cache = A.PathCache(capacity=capacity, step=sc.cell_step)
+    A.photon_trace(ds, cache, iteration=0, photons_per_triangle=ppt)
+    torch.cuda.synchronize()
+    g = cache.to_host()
+    recs = orc.photon_trace(lens_bvh, sc, iteration=0, photons_per_tri=ppt)
+    o = orc.cache_build(recs, capacity=1 << 16, step=sc.cell_step)
+    full = set(o["hash"][o["hash"] != 0].tolist())
+    used = g["hash"] != 0
+    assert used.sum() == g["count"]
+    assert 4 < len(full) < (1 << 15)
+    if capacity >= (1 << 16):
+        assert cache.status() == 0
+        assert set(g["hash"][used].tolist()) == full
+    else:
+        assert cache.status() == 0x2
+        assert used.sum() == capacity
+        assert set(g["hash"][used].tolist()) <= full
+
+
 def test_eye_pass_and_lookup(orc, lens, lens_bvh):
     sc, ds = lens
     frame = A.Frame(sc, path_capacity=1 << 22)
