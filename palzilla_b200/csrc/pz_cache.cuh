@@ -75,7 +75,7 @@ PZ_D uint32_t spacial_hash(float3 p, float step)
 }
 
 // The hash of the k-th (0..7) of the 8 cells nearest to pos, in the reference's order
-// (x fastest, then y, then z; pk.h:303-311).
+// (x fastest, then y, then z; pk.h:302-313).
 PZ_D uint32_t cache_cell_hash(const CacheView& c, float3 pos, int k)
 {
     const float3 idx = pos / c.step;
@@ -86,37 +86,54 @@ PZ_D uint32_t cache_cell_hash(const CacheView& c, float3 pos, int k)
     return hash_of_iP(x + (k & 1) * dx, y + ((k >> 1) & 1) * dy, z + (k >> 2) * dz);
 }
 
-// One cell of PathCache::store (pk.h:312-345): the probe from the cell hash's home slot.
-// It visits the same slots in the same order and stops on the same conditions as the
-// reference's CAS-per-slot loop, but reads each slot from L2 first (atomics live there):
-// a slot holding this path hash ends the probe, one holding another hash is passed, and
-// only a slot that reads empty is claimed with the CAS, whose answer is then handled
-// like the reference's.  Slots go from empty to a path hash once and never change while
-// photons are stored, so a read that saw a hash sees what the CAS would have returned.
-// t and p0/p1 are the tuple's triangle indices and barycentrics, zero past its length.
-PZ_D void cache_store_cell(const CacheView& c, uint32_t hP, uint32_t hp, uint32_t ev, int4 t, float4 p0, float4 p1)
+// A claimed slot receives the tuple (pk.h:320-339) and counts as a stored entry.
+PZ_D void cache_fill_slot(const CacheView& c, uint32_t i, uint32_t hP, uint32_t ev, int4 t, float4 p0, float4 p1)
+{
+    c.cell[i] = hP;
+    c.event[i] = ev;
+    c.tris[i] = t;
+    c.params[2 * i] = p0;
+    c.params[2 * i + 1] = p1;
+    atomicAdd(&c.h->count, 1u);
+}
+
+// One cell of PathCache::store (pk.h:313-345), probing from slot i at probe offset off
+// (the home slot, the cell hash & mask, is offset 0) for at most `steps` slots.  It visits
+// the same slots in the same order and stops on the same conditions as the reference's
+// CAS-per-slot loop, but reads each slot from L2 first (atomics live there): a slot
+// holding this path hash ends the probe, one holding another hash is passed, and only a
+// slot that reads empty is claimed with the CAS, whose answer is then handled like the
+// reference's.  Slots go from empty to a path hash once and never change while photons
+// are stored, so a read that saw a hash sees what the CAS would have returned.  t and
+// p0/p1 are the tuple's triangle indices and barycentrics, zero past its length.
+// Returns true while the probe is unfinished (i and off then name the next slot).
+PZ_D bool cache_probe(const CacheView& c, uint32_t hP, uint32_t hp, uint32_t ev, int4 t, float4 p0, float4 p1,
+                      uint32_t& i, uint32_t& off, uint32_t steps)
 {
     const uint32_t mask = c.capacity - 1u;
-    const uint32_t home = hP & mask;
-    uint32_t off = 0;
-    for (; off < kMaxProbe; off++) {
-        const uint32_t i = (home + off) & mask;
-        const uint32_t seen = __ldcg(c.hash + i);
-        if (seen == hp) break;
-        if (seen != 0u) continue;
-        const uint32_t old = atomicCAS(c.hash + i, 0u, hp);
-        if (old == 0u) {
-            c.cell[i] = hP;
-            c.event[i] = ev;
-            c.tris[i] = t;
-            c.params[2 * i] = p0;
-            c.params[2 * i + 1] = p1;
-            atomicAdd(&c.h->count, 1u);
-            break;
+    for (uint32_t k = 0; k < steps; k++) {
+        if (off >= kMaxProbe) {
+            raise_error(&c.h->status, kErrCapacity);
+            return false;
         }
-        if (old == hp) break;
+        const uint32_t seen = __ldcg(c.hash + i);
+        if (seen == hp) return false;
+        if (seen == 0u) {
+            const uint32_t old = atomicCAS(c.hash + i, 0u, hp);
+            if (old == 0u) {
+                cache_fill_slot(c, i, hP, ev, t, p0, p1);
+                return false;
+            }
+            if (old == hp) return false;
+        }
+        i = (i + 1u) & mask;
+        off++;
     }
-    if (off == kMaxProbe) raise_error(&c.h->status, kErrCapacity);
+    if (off >= kMaxProbe) {
+        raise_error(&c.h->status, kErrCapacity);
+        return false;
+    }
+    return true;
 }
 
 }  // namespace pz
