@@ -371,6 +371,7 @@ def run_ours(args):
                         "solved) over the solve stage's time; value counts every (item, bin) decided, as the "
                         "plain path decides each by a Newton solve"},
             "solve_ms_per_frame": solve_avg,
+            "solve_ms_frames": [round(float(t), 3) for t in solve_ms],
             "frame_stages": stages,
             "plain": {"value": p_value, "ms_per_frame": p_tmax / kp, "solve_ms_per_frame": float(np.mean(p_solve_ms)),
                       "steps": kp},
