@@ -13,6 +13,8 @@
   (pz_solve_desc.fma_contraction = 1) is reported against the same oracle.
 """
 import numpy as np
+
+from cache_checks import probe_reachability_violations
 import pytest
 import torch
 
@@ -101,6 +103,7 @@ def test_path_cache_contents(orc, lens, lens_bvh):
     used = g["hash"] != 0
     assert used.sum() == g["count"]
     assert set(g["hash"][used].tolist()) == set(o["hash"][o["hash"] != 0].tolist())
+    assert probe_reachability_violations(g["hash"], g["cell"], 1 << 20) == 0
     # every stored slot holds a record's tuple + barycentrics under that record's path hash
     by_hash = {}
     for r in recs:
@@ -129,6 +132,7 @@ def test_path_cache_small_tables(orc, lens, lens_bvh, capacity):
     used = g["hash"] != 0
     assert used.sum() == g["count"]
     assert 4 < len(full) < (1 << 15)
+    assert probe_reachability_violations(g["hash"], g["cell"], capacity) == 0
     if capacity >= (1 << 16):
         assert cache.status() == 0
         assert set(g["hash"][used].tolist()) == full

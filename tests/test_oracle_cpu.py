@@ -12,6 +12,8 @@
 import os
 
 import numpy as np
+
+from cache_checks import probe_reachability_violations
 import pytest
 
 import oracle as O
@@ -76,6 +78,19 @@ def test_photons_and_path_cache_bitwise(orc, g, lens):
     assert np.array_equal(used, g["cache_slots"])
     for k in ("hash", "cell", "events", "tris", "params"):
         assert c[k][used].tobytes() == g[f"cache_{k}"].tobytes(), k
+    assert probe_reachability_violations(c["hash"], c["cell"], 1 << 22) == 0
+    # a crowded table (load about 0.5, chains of tens of slots) keeps the
+    # invariant, and the check catches an entry left behind an emptied slot of its chain
+    cap = 1 << 15
+    c = orc.cache_build(recs, capacity=cap, step=lens.cell_step)
+    used = np.nonzero(c["hash"])[0]
+    assert 0.3 < used.size / cap < 0.7
+    dist = (used - (c["cell"][used] & (cap - 1))) & (cap - 1)
+    assert dist.max() > 16
+    assert probe_reachability_violations(c["hash"], c["cell"], cap) == 0
+    h = c["hash"].copy()
+    h[int(c["cell"][used[np.argmax(dist)]]) & (cap - 1)] = 0
+    assert probe_reachability_violations(h, c["cell"], cap) >= 1
 
 
 def test_solver_primitives_bitwise(orc, g, lens):
