@@ -5,10 +5,11 @@
 // linear probing from the cell hash with a CAS on the path hash; an existing equal
 // path hash stops the probe.  Lookups scan a cell's probe chain until an empty slot
 // and report slots whose cell hash and event descriptor match.  Differences: the
-// record fields live in separate arrays (probing reads 12 B per slot instead of a
-// 56-byte record), the capacity is any power of two, and a probe that exceeds
-// kMaxProbe slots stops with PZ_DEVICE_ERR_CAPACITY instead of scanning the whole
-// table.
+// record fields live in separate arrays (probing reads 4 B of path hash per slot
+// instead of a 56-byte record), a slot is read before it is claimed with the CAS (the
+// probe stops on the same slot), the capacity is any power of two, and a probe that
+// exceeds kMaxProbe slots stops with PZ_DEVICE_ERR_CAPACITY instead of scanning the
+// whole table.
 #pragma once
 #include "pz_common.cuh"
 
